@@ -1,0 +1,169 @@
+/*
+ * tmx.h -- C ABI of the B200 T-mixer solver (coupled D3Q19 lattice Boltzmann:
+ * flow plus reactive species A + B -> C in two coupled boxes).
+ *
+ * The reference (Tmixer.cpp) has no library interface: main() calls five
+ * void(void) phase functions on global arrays once per step
+ * (Tmixer.cpp:10467-10475) and fixes the case with #defines
+ * (Tmixer.cpp:76-149).  Each entry point below names the reference code it
+ * replaces.  Plain pointers and sizes only; no CUDA or torch types.
+ *
+ * Conventions
+ *   - Every function returns 0 on success or a negative TMX_E* code; the text
+ *     of the last error on the calling thread is returned by tmx_last_error().
+ *   - Boxes: 0 = inlet channel ("I", inx x iny x nz), 1 = mixing channel
+ *     ("M", mnx x mny x nz).  Host arrays are in the reference's [i][j][k]
+ *     order over nodes 1..n (k fastest), i.e. shape (nx, ny, nz) row-major.
+ *   - A handle owns all of its device memory and one CUDA stream; use one
+ *     handle from one host thread at a time.  Different handles may run
+ *     concurrently.
+ */
+#ifndef TMX_H
+#define TMX_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TMX_ABI_VERSION 1
+
+#define TMX_OK 0
+#define TMX_E_INVALID (-1)  /* invalid case or argument */
+#define TMX_E_NOMEM (-2)    /* device or host allocation failed */
+#define TMX_E_CUDA (-3)     /* CUDA runtime error */
+#define TMX_E_STATE (-4)    /* call out of order (e.g. step before init) */
+#define TMX_E_NONFINITE (-5) /* non-finite value found in the state */
+
+/* arithmetic of the state and of the step */
+#define TMX_FP64 0 /* plain form: FP64 storage and arithmetic, bit-exact with the reference */
+
+/* field ids of tmx_fields */
+#define TMX_RHO 0
+#define TMX_UX 1
+#define TMX_UY 2
+#define TMX_UZ 3
+#define TMX_CA 4
+#define TMX_CB 5
+#define TMX_CC 6
+
+/* Case parameters: the reference's compile-time constants as runtime values.
+ *   inx, iny, nz        Tmixer.cpp:122-134   inlet box size
+ *   mnx, mny            Tmixer.cpp:140-143   mixing box size
+ *   ia                  Tmixer.cpp:1374      first inlet column over the opening;
+ *                                            ib = ia + mnx - 1 (Tmixer.cpp:1375)
+ *   tau                 Tmixer.cpp:84        flow relaxation time
+ *   tau_a, tau_b, tau_c Tmixer.cpp:86-88     species relaxation times
+ *   rho0, rho_out       Tmixer.cpp:101-103   initial and outlet density
+ *   c_in[s][n]          Tmixer.cpp:90-97     species s (A,B,C) at inlet n (1,2)
+ *   rateconst           Tmixer.cpp:99        A + B -> C rate constant
+ *   umean               Tmixer.cpp:107       mean of the inlet-1 duct profile
+ *   precision           TMX_FP64
+ * Requirements: all sizes >= 3, 2 <= ia, ia + mnx - 1 <= inx - 1. */
+typedef struct tmx_case {
+    int inx, iny, nz;
+    int mnx, mny;
+    int ia;
+    double tau;
+    double tau_a, tau_b, tau_c;
+    double rho0, rho_out;
+    double c_in[3][2];
+    double rateconst;
+    double umean;
+    int precision;
+} tmx_case;
+
+typedef struct tmx_handle tmx_handle;
+
+/* ABI version of the loaded library (TMX_ABI_VERSION). */
+int tmx_abi_version(void);
+
+/* Text of the last error on the calling thread ("" if none). */
+const char *tmx_last_error(void);
+
+/* Fill *out with the reference's hard-coded case (Tmixer.cpp:76-149, with
+ * taua = taub = taup = 0.5*((2*tau-1)/3 + 1), Tmixer.cpp:86-88). */
+int tmx_case_reference(tmx_case *out);
+
+/* Fill *out with a T-mixer of width W in the layout of the benchmark
+ * configurations (no counterpart in the reference, whose sizes are fixed):
+ * inlet 8W x W x W, mixing 2W x 4W x W, opening x = 3W+1..5W, tau_a = tau_b =
+ * tau_c = tau_c, species A = 1 at inlet 1 and B = 1 at inlet 2, rho0 = rho_out
+ * = rho, rate constant k.  The reference's duct profile is scaled by mean
+ * (Umean); here umean is chosen so that the profile's maximum is u_max. */
+int tmx_case_wlayout(int W, double u_max, double tau_f, double tau_c, double k, double rho, tmx_case *out);
+
+/* Validate a case; returns TMX_E_INVALID with a message if it cannot run. */
+int tmx_case_check(const tmx_case *c);
+
+/* Device bytes tmx_create would allocate for this case. */
+int tmx_case_footprint(const tmx_case *c, long long *bytes);
+
+/* Allocate the device state of one solve on CUDA device `device`.
+ * Replaces allocateMemory() (Tmixer.cpp:711-1081). */
+int tmx_create(const tmx_case *c, int device, tmx_handle **out);
+
+/* Inlet profile, initial macroscopic state and initial distributions.
+ * Replaces GenerateInletVelocity() (Tmixer.cpp:1426-1539), initialization()
+ * (:1544-1585), equilibrium() (:1589-1831) and
+ * initialize_distribution_function() (:1835-2018). */
+int tmx_init(tmx_handle *h);
+
+/* Advance nsteps full steps.  Each step equals one pass of the reference's
+ * loop body: equilibrium, collision, streaming, boundary_conditions,
+ * calculate_velocity_density (Tmixer.cpp:10469-10475).  Asynchronous on the
+ * handle's stream; the macroscopic fields of the last step are kept. */
+int tmx_step(tmx_handle *h, int nsteps);
+
+/* Wait for all work queued on the handle. */
+int tmx_sync(tmx_handle *h);
+
+/* Number of steps completed since tmx_init. */
+long long tmx_steps_done(const tmx_handle *h);
+
+/* Copy one macroscopic field of one box after the last step into host memory
+ * (nx*ny*nz doubles).  The arrays rho/ux/uy/uz/grho/hrho/prho (and mrho, mux,
+ * ... for the mixing box) of calculate_velocity_density() (Tmixer.cpp:9352-9656),
+ * as written out by write_Domain_Data() (Tmixer.cpp:10028-10064). */
+int tmx_fields(tmx_handle *h, int box, int field, double *host_out);
+
+/* Copy the populations held between steps (post-collision, i.e. the
+ * reference's fn/gn/hn/pn arrays, Tmixer.cpp:9661-9860, that the next step
+ * streams) of field fld (0 flow, 1 A, 2 B, 3 C) of one box:
+ * 19*nx*ny*nz doubles, direction-major. */
+int tmx_populations(tmx_handle *h, int box, int fld, double *host_out);
+
+/* Mixing quality after the last step: (mny + iny) rows of
+ * {row, mean cA, mean cB, mean cC, I_A, I_B, I_C}, mixing rows 1..mny then
+ * inlet rows 1..iny over the opening; outlet_im[3] = I_A, I_B, I_C of mixing
+ * row 1 (may be NULL).  The numbers write_MixingQuality() prints
+ * (Tmixer.cpp:10161-10409), with its running maxima starting at 0. */
+int tmx_mixing(tmx_handle *h, double *rows_out, double *outlet_im);
+
+/* FP64 totals over both boxes after the last step: out[0] = sum rho,
+ * out[1..3] = sum cA, cB, cC, out[4] = sum (cA + cB + cC), out[5] = outlet
+ * flux sum(rho*uy) over mixing row 1, out[6] = number of non-finite values in
+ * the fields, out[7] = fluid nodes.  No counterpart in the reference. */
+int tmx_sums(tmx_handle *h, double out[8]);
+
+/* The inlet profiles Uin1, Uin2 as the reference keeps them
+ * ((iny+3) x (nz+3) doubles each, Tmixer.cpp:703-704). */
+int tmx_inlet_profile(tmx_handle *h, double *uin1, double *uin2);
+
+/* Run nsteps steps with CUDA events around every kernel launch on the
+ * handle's stream and return the summed device times (ms) of the bulk
+ * (interior) kernel, of the boundary kernel and of the whole step loop.
+ * Benchmark support; no counterpart in the reference. */
+int tmx_step_timed(tmx_handle *h, int nsteps, double *ms_bulk, double *ms_boundary, double *ms_total);
+
+/* Node counts: out[0] fluid nodes (both boxes), out[1] interior nodes,
+ * out[2] boundary nodes, out[3] device bytes allocated. */
+int tmx_counts(const tmx_handle *h, long long out[4]);
+
+/* Free the handle and its device memory.  Replaces deallocateMemory()
+ * (Tmixer.cpp:1083-1366). */
+void tmx_destroy(tmx_handle *h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TMX_H */

@@ -55,6 +55,8 @@ def lib():
         L.orc_pops.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
         L.orc_mixing.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         L.orc_inlet_profile.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.orc_collide_preview.argtypes = [ctypes.c_void_p]
+        L.orc_fn.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
         _lib = L
     return _lib
 
@@ -100,6 +102,15 @@ class Oracle:
         out = np.empty((19,) + self.box_shape(box), dtype=np.float64)
         for q in range(19):
             lib().orc_pops(self._h, box, fld, q, out[q].ctypes.data)
+        return out
+
+    def post_collision(self, box: int, fld: int) -> np.ndarray:
+        """The populations the next step streams (what the GPU state holds
+        between steps), shape (19, nx, ny, nz)."""
+        lib().orc_collide_preview(self._h)
+        out = np.empty((19,) + self.box_shape(box), dtype=np.float64)
+        for q in range(19):
+            lib().orc_fn(self._h, box, fld, q, out[q].ctypes.data)
         return out
 
     def mixing(self) -> np.ndarray:

@@ -1155,3 +1155,17 @@ void orc_mixing(const orc_t *S, double *rows)
 }
 
 int orc_steps_done(const orc_t *S) { return S->steps; }
+
+/* The post-collision populations the next step would stream (the next
+ * step's equilibrium + collision, Tmixer.cpp:1589-1831 and :9661-9860),
+ * left in the fn arrays; the next orc_step recomputes them identically. */
+void orc_collide_preview(orc_t *S) { collide(S); }
+
+/* post-collision population q of field fl after orc_collide_preview */
+void orc_fn(const orc_t *S, int box, int fl, int q, double *out)
+{
+    size_t o = 0;
+    for (int i = 1; i <= S->nx[box]; i++)
+        for (int j = 1; j <= S->ny[box]; j++)
+            for (int k = 1; k <= S->nz; k++) out[o++] = S->fn[box][fl][q][IX(S, box, i, j, k)];
+}

@@ -1,0 +1,43 @@
+"""The oracle against the reference binary itself, including all 76
+post-step populations of every node, on cases the fixtures do not cover.
+Runs where the reference binaries exist (built here from /root/reference by
+oracle/build_ref.py; prebuilt binaries travel with the repository)."""
+import glob
+import os
+
+import pytest
+
+from oracle import build_ref, oracle as O
+from tests.cases import GOLDEN_CASES, ref_params, ref_like, w_like
+from tests.conftest import bit_equal, first_mismatch
+
+CASES = {
+    "tiny_ref_pop": (GOLDEN_CASES["tiny_ref"][0], 9),
+    "w3_pop": (w_like(3, umean=0.04, tau=0.58, tau_c=0.7, k=0.8, rho=1.2), 25),
+    "species_pop": (GOLDEN_CASES["tiny_species"][0], 17),
+}
+
+
+def _binary(name, case):
+    path = build_ref.binary_path("t_" + name, ref_params(case))
+    if os.path.exists(path):
+        return path
+    if os.path.exists(build_ref.REF_SRC):
+        return build_ref.build("t_" + name, ref_params(case))
+    pytest.skip("reference source and prebuilt reference binary both absent")
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_oracle_populations_match_reference(name):
+    case, steps = CASES[name]
+    dump, mix, _ = O.run_ref(_binary(name, case), steps, with_pops=True, threads=2)
+    orc = O.Oracle(case)
+    orc.step(steps)
+    for b in (0, 1):
+        for f in O.FIELDS:
+            assert bit_equal(orc.field(b, f), dump[(b, f)]), (b, f, first_mismatch(orc.field(b, f), dump[(b, f)]))
+        for fld in range(4):
+            got, want = orc.pops(b, fld), dump[(b, "pops", fld)]
+            assert bit_equal(got, want), (b, fld, first_mismatch(got, want))
+    assert bit_equal(orc.mixing(), mix)
+    orc.close()

@@ -1,0 +1,275 @@
+"""tmixer_b200 -- B200-native coupled D3Q19 lattice-Boltzmann T-mixer solver.
+
+Host-side mirror of the reference's driver (Tmixer.cpp:10413-10490) over the
+C ABI of ``libtmx.so`` (``include/tmx.h``).  The reference is a single program
+whose interface is its case ``#define`` block and five phase functions; here a
+``CaseSpec`` carries the case and a ``Solver`` runs it on one GPU:
+
+    spec = tmixer_b200.reference_case()          # Tmixer.cpp:76-149
+    with tmixer_b200.Solver(spec) as s:           # allocateMemory()
+        s.init()                                  # inlet profile + initial state
+        s.step(1000)                              # 1000 x {eq, collide, stream, BC, moments}
+        rho = s.field(0, "rho")                   # inlet-box density, shape (inx, iny, nz)
+        rows, im = s.mixing()                     # write_MixingQuality numbers
+
+There is no CPU fallback: every call goes to the CUDA library, and importing
+the package fails loudly if ``libtmx.so`` is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libtmx.so")
+
+FIELDS = ("rho", "ux", "uy", "uz", "cA", "cB", "cC")
+TMX_FP64 = 0
+ABI_VERSION = 1
+
+_ERRORS = {-1: "invalid", -2: "out of memory", -3: "CUDA error", -4: "bad call order", -5: "non-finite state"}
+
+
+class TmxError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__("tmx error %d (%s): %s" % (code, _ERRORS.get(code, "?"), msg))
+        self.code = code
+
+
+class _CCase(ctypes.Structure):
+    _fields_ = [("inx", ctypes.c_int), ("iny", ctypes.c_int), ("nz", ctypes.c_int),
+                ("mnx", ctypes.c_int), ("mny", ctypes.c_int), ("ia", ctypes.c_int),
+                ("tau", ctypes.c_double), ("tau_a", ctypes.c_double), ("tau_b", ctypes.c_double),
+                ("tau_c", ctypes.c_double), ("rho0", ctypes.c_double), ("rho_out", ctypes.c_double),
+                ("c_in", (ctypes.c_double * 2) * 3), ("rateconst", ctypes.c_double),
+                ("umean", ctypes.c_double), ("precision", ctypes.c_int)]
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load ``libtmx.so`` (built by ``tmixer_b200.build``); raises if absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError("tmixer_b200: %s is missing; run `python -m tmixer_b200.build`" % LIB_PATH)
+    L = ctypes.CDLL(LIB_PATH)
+    P = ctypes.POINTER
+    vp, ip, dp = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+    L.tmx_abi_version.restype = ip
+    L.tmx_last_error.restype = ctypes.c_char_p
+    L.tmx_case_reference.argtypes = [P(_CCase)]
+    L.tmx_case_check.argtypes = [P(_CCase)]
+    L.tmx_case_footprint.argtypes = [P(_CCase), P(ctypes.c_longlong)]
+    L.tmx_case_wlayout.argtypes = [ip, dp, dp, dp, dp, dp, P(_CCase)]
+    L.tmx_create.argtypes = [P(_CCase), ip, P(vp)]
+    L.tmx_init.argtypes = [vp]
+    L.tmx_step.argtypes = [vp, ip]
+    L.tmx_sync.argtypes = [vp]
+    L.tmx_steps_done.argtypes = [vp]
+    L.tmx_steps_done.restype = ctypes.c_longlong
+    L.tmx_fields.argtypes = [vp, ip, ip, vp]
+    L.tmx_populations.argtypes = [vp, ip, ip, vp]
+    L.tmx_mixing.argtypes = [vp, vp, vp]
+    L.tmx_sums.argtypes = [vp, vp]
+    L.tmx_inlet_profile.argtypes = [vp, vp, vp]
+    L.tmx_step_timed.argtypes = [vp, ip, P(dp), P(dp), P(dp)]
+    L.tmx_counts.argtypes = [vp, P(ctypes.c_longlong)]
+    L.tmx_destroy.argtypes = [vp]
+    L.tmx_destroy.restype = None
+    if L.tmx_abi_version() != ABI_VERSION:
+        raise RuntimeError("libtmx.so ABI %d, expected %d" % (L.tmx_abi_version(), ABI_VERSION))
+    _lib = L
+    return L
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        raise TmxError(rc, lib().tmx_last_error().decode(errors="replace"))
+
+
+@dataclasses.dataclass
+class CaseSpec:
+    """The reference's case constants (Tmixer.cpp:76-149) as runtime values.
+
+    ``ia`` is the first inlet column over the opening; the last is
+    ``ib = ia + mnx - 1`` (Tmixer.cpp:1374-1375).  ``c_in[s][n]`` is species s
+    (A, B, C) at inlet n (1, 2).
+    """
+    inx: int
+    iny: int
+    nz: int
+    mnx: int
+    mny: int
+    ia: int
+    tau: float
+    tau_a: float
+    tau_b: float
+    tau_c: float
+    rho0: float
+    rho_out: float
+    c_in: Sequence[Sequence[float]]
+    rateconst: float
+    umean: float
+    precision: int = TMX_FP64
+    steps: int = 0  # the case's step count (the reference loops time+1 = 100001 times)
+
+    @property
+    def ib(self) -> int:
+        return self.ia + self.mnx - 1
+
+    def nodes(self) -> int:
+        return self.inx * self.iny * self.nz + self.mnx * self.mny * self.nz
+
+    def to_c(self) -> _CCase:
+        c = _CCase()
+        for k in ("inx", "iny", "nz", "mnx", "mny", "ia", "precision"):
+            setattr(c, k, int(getattr(self, k)))
+        for k in ("tau", "tau_a", "tau_b", "tau_c", "rho0", "rho_out", "rateconst", "umean"):
+            setattr(c, k, float(getattr(self, k)))
+        for s in range(3):
+            for n in range(2):
+                c.c_in[s][n] = float(self.c_in[s][n])
+        return c
+
+    @classmethod
+    def from_c(cls, c: _CCase, steps: int = 0) -> "CaseSpec":
+        return cls(inx=c.inx, iny=c.iny, nz=c.nz, mnx=c.mnx, mny=c.mny, ia=c.ia, tau=c.tau, tau_a=c.tau_a,
+                   tau_b=c.tau_b, tau_c=c.tau_c, rho0=c.rho0, rho_out=c.rho_out,
+                   c_in=[[c.c_in[s][n] for n in range(2)] for s in range(3)], rateconst=c.rateconst,
+                   umean=c.umean, precision=c.precision, steps=steps)
+
+    def as_dict(self) -> dict:
+        """Plain-dict form (the oracle's parameter names)."""
+        return dict(inx=self.inx, iny=self.iny, nz=self.nz, mnx=self.mnx, mny=self.mny, ia=self.ia,
+                    tau=self.tau, taua=self.tau_a, taub=self.tau_b, taup=self.tau_c, rho0=self.rho0,
+                    rho_out=self.rho_out, c0=0.0, cin=[list(r) for r in self.c_in],
+                    rateconst=self.rateconst, umean=self.umean)
+
+    def check(self) -> None:
+        _check(lib().tmx_case_check(ctypes.byref(self.to_c())))
+
+    def footprint(self) -> int:
+        b = ctypes.c_longlong()
+        _check(lib().tmx_case_footprint(ctypes.byref(self.to_c()), ctypes.byref(b)))
+        return int(b.value)
+
+
+def reference_case() -> CaseSpec:
+    """The reference's hard-coded case: 401x51x51 inlet box, 101x750x51 mixing
+    box, tau 0.6, Sc 3, Umean 0.059761, k 1.0, rho 3.0, 100001 steps."""
+    c = _CCase()
+    _check(lib().tmx_case_reference(ctypes.byref(c)))
+    return CaseSpec.from_c(c, steps=100001)
+
+
+def w_layout(W: int, u_max: float, tau_f: float, tau_c: float, k: float, rho: float = 1.0,
+             steps: int = 0) -> CaseSpec:
+    """A T-mixer of width W in the layout of the benchmark configurations:
+    inlet 8W x W x W, mixing 2W x 4W x W, opening x = 3W+1 .. 5W, species A
+    at inlet 1 and B at inlet 2 with c = 1, rho0 = rho_out = rho.  The duct
+    profile is scaled so that its maximum is u_max (instead of the reference's
+    mean Umean): umean is set to u_max * mean/max of the unscaled profile."""
+    c = _CCase()
+    _check(lib().tmx_case_wlayout(int(W), float(u_max), float(tau_f), float(tau_c), float(k), float(rho),
+                                  ctypes.byref(c)))
+    return CaseSpec.from_c(c, steps=steps)
+
+
+class Solver:
+    """One solve on one GPU: the device state of a ``CaseSpec``."""
+
+    def __init__(self, spec: CaseSpec, device: int = 0):
+        self.spec = spec
+        self._h = ctypes.c_void_p()
+        self._c = spec.to_c()
+        _check(lib().tmx_create(ctypes.byref(self._c), int(device), ctypes.byref(self._h)))
+
+    # -- lifecycle ---------------------------------------------------------
+    def init(self) -> "Solver":
+        _check(lib().tmx_init(self._h))
+        return self
+
+    def step(self, n: int = 1) -> "Solver":
+        _check(lib().tmx_step(self._h, int(n)))
+        return self
+
+    def sync(self) -> None:
+        _check(lib().tmx_sync(self._h))
+
+    @property
+    def steps_done(self) -> int:
+        return int(lib().tmx_steps_done(self._h))
+
+    def close(self) -> None:
+        if self._h:
+            lib().tmx_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- outputs -------------------------------------------------------------
+    def box_shape(self, box: int):
+        s = self.spec
+        return (s.inx, s.iny, s.nz) if box == 0 else (s.mnx, s.mny, s.nz)
+
+    def field(self, box: int, name: str, out: Optional[np.ndarray] = None) -> np.ndarray:
+        if out is None:
+            out = np.empty(self.box_shape(box), dtype=np.float64)
+        assert out.dtype == np.float64 and out.flags.c_contiguous and out.shape == self.box_shape(box)
+        _check(lib().tmx_fields(self._h, int(box), FIELDS.index(name), out.ctypes.data))
+        return out
+
+    def populations(self, box: int, fld: int) -> np.ndarray:
+        out = np.empty((19,) + self.box_shape(box), dtype=np.float64)
+        _check(lib().tmx_populations(self._h, int(box), int(fld), out.ctypes.data))
+        return out
+
+    def mixing(self):
+        rows = np.empty((self.spec.mny + self.spec.iny, 7), dtype=np.float64)
+        im = np.empty(3, dtype=np.float64)
+        _check(lib().tmx_mixing(self._h, rows.ctypes.data, im.ctypes.data))
+        return rows, im
+
+    def sums(self) -> np.ndarray:
+        out = np.empty(8, dtype=np.float64)
+        _check(lib().tmx_sums(self._h, out.ctypes.data))
+        return out
+
+    def inlet_profile(self):
+        n = (self.spec.iny + 3, self.spec.nz + 3)
+        u1 = np.empty(n, dtype=np.float64)
+        u2 = np.empty(n, dtype=np.float64)
+        _check(lib().tmx_inlet_profile(self._h, u1.ctypes.data, u2.ctypes.data))
+        return u1, u2
+
+    def step_timed(self, n: int):
+        """Run n steps with CUDA events around every launch; returns
+        (ms in the bulk kernel, ms in the boundary kernel, ms for the loop)."""
+        a, b, t = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        _check(lib().tmx_step_timed(self._h, int(n), ctypes.byref(a), ctypes.byref(b), ctypes.byref(t)))
+        return a.value, b.value, t.value
+
+    def counts(self) -> dict:
+        o = (ctypes.c_longlong * 4)()
+        _check(lib().tmx_counts(self._h, o))
+        return dict(nodes=o[0], interior=o[1], boundary=o[2], device_bytes=o[3])
+
+
+__all__ = ["CaseSpec", "Solver", "TmxError", "FIELDS", "reference_case", "w_layout", "lib"]

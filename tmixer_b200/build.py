@@ -1,0 +1,58 @@
+"""Build the in-tree CUDA library ``tmixer_b200/libtmx.so`` (sm_100a) and the
+C++ driver ``tmixer_b200/tmx_run``.
+
+nvcc cross-compiles without a GPU.  ``--fmad=false`` keeps every multiply and
+add separately rounded (the reference is built for x86-64 without FMA
+contraction); the kernels fuse only where they say so with ``__fma_rn``.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+LIB = os.path.join(PKG, "libtmx.so")
+RUN = os.path.join(PKG, "tmx_run")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC"]
+SOURCES = ["tmx_kernels.cu", "tmx_api.cu"]
+
+
+def _nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", "nvcc"):
+        if cand and (os.path.sep not in cand or os.path.exists(cand)):
+            return cand
+    return "nvcc"
+
+
+def _stale(target: str, deps: list[str]) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    srcs = [os.path.join(CSRC, s) for s in SOURCES]
+    deps = srcs + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
+    deps.append(os.path.join(ROOT, "include", "tmx.h"))
+    if force or _stale(LIB, deps):
+        tmp = LIB + ".tmp"
+        cmd = [_nvcc()] + NVCC_FLAGS + ARCH + ["-shared", "-o", tmp] + srcs
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True)
+        os.replace(tmp, LIB)
+    drv = os.path.join(CSRC, "tmx_run.cpp")
+    if os.path.exists(drv) and (force or _stale(RUN, [drv, LIB])):
+        cmd = ["g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), drv, "-o", RUN,
+               "-L", PKG, "-ltmx", "-Wl,-rpath,$ORIGIN"]
+        subprocess.run(cmd, check=True)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose=True))

@@ -1,0 +1,635 @@
+// tmx_api.cu -- host side of the C ABI declared in include/tmx.h.
+//
+// Owns the device state of one T-mixer solve: two population buffers (A-B
+// pull), two density buffers (previous / current step, read by boundary
+// closures), the macroscopic fields of the last step, the compact boundary
+// node list and the inlet profiles.  Kernels are in tmx_kernels.cu.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/tmx.h"
+#include "tmx_classes.h"
+#include "tmx_kernels.cuh"
+
+using tmx::Geom;
+using tmx::Phys;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define TMX_CK(call)                                                                                    \
+    do {                                                                                                \
+        cudaError_t e_ = (call);                                                                        \
+        if (e_ != cudaSuccess) return fail(TMX_E_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                                           __FILE__, __LINE__);                                         \
+    } while (0)
+
+}  // namespace
+
+struct tmx_handle {
+    tmx_case c;
+    Geom G;
+    Phys P;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    double* pop[2] = {nullptr, nullptr};
+    double* rho[2] = {nullptr, nullptr};
+    double* mac = nullptr;
+    int* bnode = nullptr;
+    unsigned char* bcls = nullptr;
+    int nb = 0;
+    double* uin_d[2] = {nullptr, nullptr};
+    double* stats = nullptr;
+    double* partial = nullptr;
+    std::vector<double> uin1, uin2;
+    std::vector<int> class_count;
+    int cur = 0;   // population buffer holding the state
+    int rcur = 0;  // density buffer holding the previous step's densities
+    long long steps = 0;
+    bool inited = false;
+    long long bytes = 0;
+    int bulk_blocks = 0;
+};
+
+namespace {
+
+constexpr int kSumBlocks = 592;
+
+void geometry_of(const tmx_case& c, Geom& G)
+{
+    G.inx = c.inx;
+    G.iny = c.iny;
+    G.nz = c.nz;
+    G.mnx = c.mnx;
+    G.mny = c.mny;
+    G.ia = c.ia;
+    G.ib = c.ia + c.mnx - 1;
+    G.nx[0] = c.inx;
+    G.ny[0] = c.iny;
+    G.nx[1] = c.mnx;
+    G.ny[1] = c.mny;
+    G.base[0] = 0;
+    G.base[1] = c.inx * c.iny * c.nz;
+    G.nnodes = G.base[1] + c.mnx * c.mny * c.nz;
+    G.ps = ((long long)G.nnodes + 63) / 64 * 64;
+}
+
+void physics_of(const tmx_case& c, Phys& P)
+{
+    const double taus[4] = {c.tau, c.tau_a, c.tau_b, c.tau_c};
+    for (int f = 0; f < 4; f++) {
+        P.c1[f] = (1.0 - 1.0 / taus[f]);  // Tmixer.cpp:9677 "(1.0 - 1.0 / tau)"
+        P.c2[f] = (1.0 / taus[f]);
+    }
+    P.rateconst = c.rateconst;
+    P.rho_out = c.rho_out;
+    for (int s = 0; s < 3; s++)
+        for (int n = 0; n < 2; n++) P.cin[s][n] = c.c_in[s][n];
+}
+
+long long footprint(const Geom& G, long long nb)
+{
+    long long b = 0;
+    b += 2LL * 76 * G.ps * 8;  // populations
+    b += 2LL * 4 * G.ps * 8;   // densities
+    b += 7LL * G.ps * 8;       // macroscopic fields
+    b += nb * 5;               // boundary list
+    b += 2LL * (G.iny + 3) * (G.nz + 3) * 8;
+    b += (long long)(G.mny + G.iny) * 9 * 8 + kSumBlocks * 6 * 8;
+    return b;
+}
+
+long long boundary_count(const Geom& G)
+{
+    long long n = 0;
+    for (int b = 0; b < 2; b++)
+        for (int i = 1; i <= G.nx[b]; i++)
+            for (int j = 1; j <= G.ny[b]; j++)
+                for (int k = 1; k <= G.nz; k++) n += tmx::is_boundary(G, b, i, j, k);
+    return n;
+}
+
+// Class of a boundary node, following the node sets of the reference's cases
+// (Tmixer.cpp:2023-9033).  Returns -1 for a node no case covers.
+int classify(const Geom& G, int b, int i, int j, int k)
+{
+    using namespace tmx;
+    const int nz = G.nz;
+    const bool zlo = k == 1, zhi = k == nz, zmid = !zlo && !zhi;
+    if (b == 0) {
+        const int inx = G.inx, iny = G.iny, ia = G.ia, ib = G.ib;
+        const bool ylo = j == 1, yhi = j == iny, ymid = !ylo && !yhi;
+        if (i == 1 || i == inx) {
+            const bool lo = i == 1;
+            if (ylo) return zlo ? (lo ? K_CORNER_1 + 6 : K_CORNER_1 + 7) : zhi ? (lo ? K_CORNER_1 + 2 : K_CORNER_1 + 3)
+                                                                              : (lo ? K_EDGE_X1_Y1 : K_EDGE_XT_Y1);
+            if (yhi) return zlo ? (lo ? K_CORNER_1 + 4 : K_CORNER_1 + 5) : zhi ? (lo ? K_CORNER_1 + 0 : K_CORNER_1 + 1)
+                                                                              : (lo ? K_EDGE_X1_YT : K_EDGE_XT_YT);
+            return zlo ? (lo ? K_EDGE_X1_Z1 : K_EDGE_XT_Z1) : zhi ? (lo ? K_EDGE_X1_ZTOP : K_EDGE_XT_ZTOP)
+                                                                 : (lo ? K_INLET1 : K_INLET2);
+        }
+        if (yhi) return zlo ? K_EDGE_YT_Z1 : zhi ? K_EDGE_YT_ZT : K_FACE_YT;
+        if (ylo) {
+            if (i < ia || i > ib) return zlo ? K_EDGE_Y1_Z1 : zhi ? K_EDGE_Y1_ZTOP : K_FACE_Y1;
+            if (i == ia) return zlo ? K_CORNER_1 + 15 : zhi ? K_CORNER_1 + 12 : K_JUNC_DD;
+            if (i == ib) return zlo ? K_CORNER_1 + 14 : zhi ? K_CORNER_1 + 13 : K_JUNC_CC;
+            return zlo ? K_FACE_Z1 : zhi ? K_FACE_ZT : -1;  // opening nodes of Cases 19 / 17
+        }
+        (void)ymid;
+        if (zlo) return K_FACE_Z1;
+        if (zhi) return K_FACE_ZT;
+        return -1;
+    }
+    const int mnx = G.mnx;
+    const bool xlo = i == 1, xhi = i == mnx;
+    if (j == 1) {
+        if (xlo) return zlo ? K_CORNER_1 + 8 : zhi ? K_CORNER_1 + 10 : K_MEDGE_AAp;
+        if (xhi) return zlo ? K_CORNER_1 + 9 : zhi ? K_CORNER_1 + 11 : K_MEDGE_BBp;
+        return zlo ? K_MEDGE_AB : zhi ? K_MEDGE_ApBp : K_OUTLET;
+    }
+    if (xlo) return zlo ? K_MEDGE_AD : zhi ? K_MEDGE_ApDp : K_FACE_MX1;
+    if (xhi) return zlo ? K_MEDGE_BC : zhi ? K_MEDGE_BpCp : K_FACE_MXT;
+    if (zlo) return K_FACE_Z1;
+    if (zhi) return K_FACE_ZT;
+    (void)zmid;
+    return -1;
+}
+
+// Inlet profiles exactly as GenerateInletVelocity() (Tmixer.cpp:1426-1539)
+// computes them: a rectangular-duct series (100 x 100 terms, libm sin/cos,
+// the same loop nesting and operation order), scaled to mean umean, then
+// shifted one node down in z (Uin1) and, negated, one node up (Uin2), with
+// Uin1[.][1] and Uin2[.][nz] zeroed.
+void inlet_profile(const tmx_case& c, std::vector<double>& U1, std::vector<double>& U2)
+{
+    const int iny = c.iny, nz = c.nz, W = nz + 3;
+    U1.assign((size_t)(iny + 3) * W, 0.0);
+    U2.assign((size_t)(iny + 3) * W, 0.0);
+    auto at = [W](std::vector<double>& a, int j, int k) -> double& { return a[(size_t)j * W + k]; };
+    const double pi = 3.14159265358979323846;
+    const double d = ((nz - 1.0) / 2.0);
+    const double w = ((iny - 1.0) / 2.0);
+    const double AR = (1.0 * w / d);
+    const double den_m = 2.0 * AR * d, den_n = 2.0 * d, AR2 = AR * AR;
+    for (int j = 0; j < iny; j++)
+        for (int k = 0; k < nz; k++) {
+            double nsum = 0;
+            for (int n = 1; n <= 100; n++) {
+                double msum = 0;
+                for (int m = 1; m <= 100; m++) {
+                    const double N = (1.0 - std::cos(m * pi)) * (1.0 - std::cos(n * pi)) *
+                                     std::sin(((m * pi) / den_m) * (j)) * std::sin(((n * pi) / den_n) * (k));
+                    const double D = m * n * ((m * m) + (AR2 * n * n));
+                    msum += (N / D);
+                }
+                nsum += msum;
+            }
+            at(U1, j + 1, k + 1) = nsum;
+        }
+    double sum = 0;
+    for (int i = 1; i <= iny; i++)
+        for (int j = 1; j <= nz; j++) sum += at(U1, i, j);
+    const double average = sum / ((iny) * (nz));
+    for (int i = 1; i <= iny; i++)
+        for (int j = 1; j <= nz; j++) at(U1, i, j) = at(U1, i, j) * (c.umean / average);
+    for (int j = 0; j < iny; j++)
+        for (int k = 0; k < nz; k++) {
+            at(U1, j + 1, k) = at(U1, j + 1, k + 1);
+            at(U2, j + 1, k + 2) = -at(U1, j + 1, k);
+        }
+    for (int i = 1; i <= iny; i++) {
+        at(U1, i, 1) = 0;
+        at(U2, i, nz) = 0;
+    }
+}
+
+void free_all(tmx_handle* h)
+{
+    for (int s = 0; s < 2; s++) {
+        cudaFree(h->pop[s]);
+        cudaFree(h->rho[s]);
+        cudaFree(h->uin_d[s]);
+        h->pop[s] = h->rho[s] = h->uin_d[s] = nullptr;
+    }
+    cudaFree(h->mac);
+    cudaFree(h->bnode);
+    cudaFree(h->bcls);
+    cudaFree(h->stats);
+    cudaFree(h->partial);
+    h->mac = h->stats = h->partial = nullptr;
+    h->bnode = nullptr;
+    h->bcls = nullptr;
+    if (h->stream) cudaStreamDestroy(h->stream);
+    h->stream = nullptr;
+}
+
+int launch_step(tmx_handle* h, int write_macro, cudaEvent_t* ev /* 3 events or null */)
+{
+    const Geom& G = h->G;
+    const double* pin = h->pop[h->cur];
+    double* pout = h->pop[1 - h->cur];
+    const double* rprev = h->rho[h->rcur];
+    double* rcur = h->rho[1 - h->rcur];
+    if (ev) TMX_CK(cudaEventRecord(ev[0], h->stream));
+    tmx::k_bulk<<<h->bulk_blocks, 256, 0, h->stream>>>(pin, pout, rcur, h->mac, G, h->P, write_macro);
+    if (ev) TMX_CK(cudaEventRecord(ev[1], h->stream));
+    if (h->nb > 0)
+        tmx::k_boundary<<<(h->nb + 127) / 128, 128, 0, h->stream>>>(pin, pout, rprev, rcur, h->mac, h->bnode, h->bcls,
+                                                                   h->nb, h->uin_d[0], h->uin_d[1], G, h->P,
+                                                                   write_macro);
+    if (ev) TMX_CK(cudaEventRecord(ev[2], h->stream));
+    TMX_CK(cudaGetLastError());
+    h->cur = 1 - h->cur;
+    h->rcur = 1 - h->rcur;
+    h->steps++;
+    return TMX_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tmx_abi_version(void) { return TMX_ABI_VERSION; }
+
+const char* tmx_last_error(void) { return g_err.c_str(); }
+
+int tmx_case_reference(tmx_case* out)
+{
+    if (!out) return fail(TMX_E_INVALID, "tmx_case_reference: null output");
+    std::memset(out, 0, sizeof *out);
+    out->inx = 401;
+    out->iny = 51;
+    out->nz = 51;
+    out->mnx = 101;
+    out->mny = 800 - 50;
+    out->ia = ((401 + 1) / 2) - ((101 - 1) / 2);
+    out->tau = 0.6;
+    const double tc = (0.5 * (((2.0 * 0.6 - 1.0) / 3.0) + 1.0));
+    out->tau_a = out->tau_b = out->tau_c = tc;
+    out->rho0 = 3.0;
+    out->rho_out = 3.0;
+    out->c_in[0][0] = 1.0;
+    out->c_in[1][1] = 1.0;
+    out->rateconst = 1.0;
+    out->umean = 0.059761;
+    out->precision = TMX_FP64;
+    return TMX_OK;
+}
+
+int tmx_case_wlayout(int W, double u_max, double tau_f, double tau_c, double k, double rho, tmx_case* out)
+{
+    if (!out) return fail(TMX_E_INVALID, "tmx_case_wlayout: null output");
+    if (W < 3) return fail(TMX_E_INVALID, "tmx_case_wlayout: W=%d must be >= 3", W);
+    if (!(u_max > 0) || !std::isfinite(u_max)) return fail(TMX_E_INVALID, "u_max must be positive");
+    tmx_case c;
+    std::memset(&c, 0, sizeof c);
+    c.inx = 8 * W;
+    c.iny = W;
+    c.nz = W;
+    c.mnx = 2 * W;
+    c.mny = 4 * W;
+    c.ia = 3 * W + 1;
+    c.tau = tau_f;
+    c.tau_a = c.tau_b = c.tau_c = tau_c;
+    c.rho0 = rho;
+    c.rho_out = rho;
+    c.c_in[0][0] = 1.0;
+    c.c_in[1][1] = 1.0;
+    c.rateconst = k;
+    c.umean = 1.0;
+    c.precision = TMX_FP64;
+    std::vector<double> U1, U2;
+    inlet_profile(c, U1, U2);
+    double mx = 0.0;
+    for (double v : U1) mx = std::max(mx, v);
+    if (!(mx > 0)) return fail(TMX_E_INVALID, "degenerate inlet profile");
+    c.umean = u_max / mx;
+    *out = c;
+    return tmx_case_check(out);
+}
+
+int tmx_case_check(const tmx_case* c)
+{
+    if (!c) return fail(TMX_E_INVALID, "null case");
+    if (c->inx < 3 || c->iny < 3 || c->nz < 3 || c->mnx < 3 || c->mny < 3)
+        return fail(TMX_E_INVALID, "every box size must be >= 3 (inx=%d iny=%d nz=%d mnx=%d mny=%d)", c->inx, c->iny,
+                    c->nz, c->mnx, c->mny);
+    if (c->ia < 2 || c->ia + c->mnx - 1 > c->inx - 1)
+        return fail(TMX_E_INVALID, "opening columns ia=%d..ib=%d must lie within 2..inx-1=%d", c->ia,
+                    c->ia + c->mnx - 1, c->inx - 1);
+    const double t[4] = {c->tau, c->tau_a, c->tau_b, c->tau_c};
+    for (double v : t)
+        if (!(v > 0.5) || !std::isfinite(v)) return fail(TMX_E_INVALID, "relaxation times must be finite and > 0.5");
+    if (!std::isfinite(c->rho0) || !(c->rho0 > 0) || !std::isfinite(c->rho_out) || !(c->rho_out > 0))
+        return fail(TMX_E_INVALID, "rho0 and rho_out must be finite and positive");
+    if (!std::isfinite(c->umean) || !std::isfinite(c->rateconst)) return fail(TMX_E_INVALID, "non-finite parameter");
+    if (c->precision != TMX_FP64) return fail(TMX_E_INVALID, "unsupported precision %d", c->precision);
+    const long long n = (long long)c->inx * c->iny * c->nz + (long long)c->mnx * c->mny * c->nz;
+    if (n > 2000000000LL / 1) return fail(TMX_E_INVALID, "too many nodes (%lld)", n);
+    return TMX_OK;
+}
+
+int tmx_case_footprint(const tmx_case* c, long long* bytes)
+{
+    int rc = tmx_case_check(c);
+    if (rc) return rc;
+    if (!bytes) return fail(TMX_E_INVALID, "null output");
+    Geom G;
+    geometry_of(*c, G);
+    *bytes = footprint(G, boundary_count(G));
+    return TMX_OK;
+}
+
+int tmx_create(const tmx_case* c, int device, tmx_handle** out)
+{
+    if (!out) return fail(TMX_E_INVALID, "null output handle");
+    *out = nullptr;
+    int rc = tmx_case_check(c);
+    if (rc) return rc;
+    int ndev = 0;
+    TMX_CK(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev) return fail(TMX_E_INVALID, "device %d out of range (%d devices)", device, ndev);
+    TMX_CK(cudaSetDevice(device));
+
+    tmx_handle* h = new tmx_handle();
+    h->c = *c;
+    h->device = device;
+    geometry_of(*c, h->G);
+    physics_of(*c, h->P);
+    const Geom& G = h->G;
+
+    // boundary node list, sorted by class then node index
+    std::vector<std::pair<int, int>> bl;
+    bl.reserve((size_t)boundary_count(G));
+    h->class_count.assign(tmx::K_NCLASSES, 0);
+    for (int b = 0; b < 2; b++)
+        for (int i = 1; i <= G.nx[b]; i++)
+            for (int j = 1; j <= G.ny[b]; j++)
+                for (int k = 1; k <= G.nz; k++) {
+                    if (!tmx::is_boundary(G, b, i, j, k)) continue;
+                    const int cls = classify(G, b, i, j, k);
+                    if (cls < 0) {
+                        delete h;
+                        return fail(TMX_E_INVALID, "internal: boundary node (%d,%d,%d,%d) has no class", b, i, j, k);
+                    }
+                    bl.emplace_back(cls, tmx::node_index(G, b, i, j, k));
+                    h->class_count[cls]++;
+                }
+    std::sort(bl.begin(), bl.end());
+    h->nb = (int)bl.size();
+    std::vector<int> nodes(bl.size());
+    std::vector<unsigned char> cls(bl.size());
+    for (size_t t = 0; t < bl.size(); t++) {
+        cls[t] = (unsigned char)bl[t].first;
+        nodes[t] = bl[t].second;
+    }
+
+    auto alloc = [&](void** p, size_t n) -> cudaError_t {
+        cudaError_t e = cudaMalloc(p, n);
+        if (e == cudaSuccess) h->bytes += (long long)n;
+        return e;
+    };
+    cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    for (int s = 0; s < 2 && e == cudaSuccess; s++) {
+        e = alloc((void**)&h->pop[s], (size_t)76 * G.ps * sizeof(double));
+        if (e == cudaSuccess) e = alloc((void**)&h->rho[s], (size_t)4 * G.ps * sizeof(double));
+        if (e == cudaSuccess) e = alloc((void**)&h->uin_d[s], (size_t)(G.iny + 3) * (G.nz + 3) * sizeof(double));
+    }
+    if (e == cudaSuccess) e = alloc((void**)&h->mac, (size_t)7 * G.ps * sizeof(double));
+    if (e == cudaSuccess) e = alloc((void**)&h->bnode, std::max<size_t>(1, nodes.size()) * sizeof(int));
+    if (e == cudaSuccess) e = alloc((void**)&h->bcls, std::max<size_t>(1, cls.size()));
+    if (e == cudaSuccess) e = alloc((void**)&h->stats, (size_t)(G.mny + G.iny) * 9 * sizeof(double));
+    if (e == cudaSuccess) e = alloc((void**)&h->partial, (size_t)kSumBlocks * 6 * sizeof(double));
+    if (e == cudaSuccess && h->nb)
+        e = cudaMemcpy(h->bnode, nodes.data(), nodes.size() * sizeof(int), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && h->nb) e = cudaMemcpy(h->bcls, cls.data(), cls.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        const int code = (e == cudaErrorMemoryAllocation) ? TMX_E_NOMEM : TMX_E_CUDA;
+        free_all(h);
+        delete h;
+        cudaGetLastError();
+        return fail(code, "tmx_create: %s", cudaGetErrorString(e));
+    }
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    h->bulk_blocks = std::max(1, std::min((G.nnodes + 255) / 256, sms * 8));
+    *out = h;
+    return TMX_OK;
+}
+
+int tmx_init(tmx_handle* h)
+{
+    if (!h) return fail(TMX_E_INVALID, "null handle");
+    TMX_CK(cudaSetDevice(h->device));
+    inlet_profile(h->c, h->uin1, h->uin2);
+    const size_t nu = h->uin1.size() * sizeof(double);
+    TMX_CK(cudaMemcpyAsync(h->uin_d[0], h->uin1.data(), nu, cudaMemcpyHostToDevice, h->stream));
+    TMX_CK(cudaMemcpyAsync(h->uin_d[1], h->uin2.data(), nu, cudaMemcpyHostToDevice, h->stream));
+    h->cur = 0;
+    h->rcur = 0;
+    tmx::k_init<<<h->bulk_blocks, 256, 0, h->stream>>>(h->pop[0], h->rho[0], h->mac, h->G, h->P, h->c.rho0);
+    TMX_CK(cudaGetLastError());
+    TMX_CK(cudaStreamSynchronize(h->stream));
+    h->steps = 0;
+    h->inited = true;
+    return TMX_OK;
+}
+
+int tmx_step(tmx_handle* h, int nsteps)
+{
+    if (!h) return fail(TMX_E_INVALID, "null handle");
+    if (!h->inited) return fail(TMX_E_STATE, "tmx_step before tmx_init");
+    if (nsteps < 0) return fail(TMX_E_INVALID, "negative step count");
+    TMX_CK(cudaSetDevice(h->device));
+    for (int s = 0; s < nsteps; s++) {
+        int rc = launch_step(h, s == nsteps - 1, nullptr);
+        if (rc) return rc;
+    }
+    return TMX_OK;
+}
+
+int tmx_sync(tmx_handle* h)
+{
+    if (!h) return fail(TMX_E_INVALID, "null handle");
+    TMX_CK(cudaSetDevice(h->device));
+    TMX_CK(cudaStreamSynchronize(h->stream));
+    return TMX_OK;
+}
+
+long long tmx_steps_done(const tmx_handle* h) { return h ? h->steps : -1; }
+
+int tmx_fields(tmx_handle* h, int box, int field, double* host_out)
+{
+    if (!h || !host_out) return fail(TMX_E_INVALID, "null argument");
+    if (box < 0 || box > 1 || field < 0 || field > 6) return fail(TMX_E_INVALID, "box %d / field %d out of range", box, field);
+    if (!h->inited) return fail(TMX_E_STATE, "tmx_fields before tmx_init");
+    TMX_CK(cudaSetDevice(h->device));
+    const Geom& G = h->G;
+    const size_t n = (size_t)G.nx[box] * G.ny[box] * G.nz;
+    TMX_CK(cudaMemcpyAsync(host_out, h->mac + (size_t)field * G.ps + G.base[box], n * sizeof(double),
+                           cudaMemcpyDeviceToHost, h->stream));
+    TMX_CK(cudaStreamSynchronize(h->stream));
+    return TMX_OK;
+}
+
+int tmx_populations(tmx_handle* h, int box, int fld, double* host_out)
+{
+    if (!h || !host_out) return fail(TMX_E_INVALID, "null argument");
+    if (box < 0 || box > 1 || fld < 0 || fld > 3) return fail(TMX_E_INVALID, "box %d / field %d out of range", box, fld);
+    if (!h->inited) return fail(TMX_E_STATE, "tmx_populations before tmx_init");
+    TMX_CK(cudaSetDevice(h->device));
+    const Geom& G = h->G;
+    const size_t n = (size_t)G.nx[box] * G.ny[box] * G.nz;
+    for (int q = 0; q < 19; q++)
+        TMX_CK(cudaMemcpyAsync(host_out + q * n, h->pop[h->cur] + (size_t)(fld * 19 + q) * G.ps + G.base[box],
+                               n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    TMX_CK(cudaStreamSynchronize(h->stream));
+    return TMX_OK;
+}
+
+int tmx_mixing(tmx_handle* h, double* rows_out, double* outlet_im)
+{
+    if (!h || !rows_out) return fail(TMX_E_INVALID, "null argument");
+    if (!h->inited) return fail(TMX_E_STATE, "tmx_mixing before tmx_init");
+    TMX_CK(cudaSetDevice(h->device));
+    const Geom& G = h->G;
+    const int nrow = G.mny + G.iny;
+    tmx::k_mixing_rows<<<nrow, 32, 0, h->stream>>>(h->mac, G, h->stats);
+    TMX_CK(cudaGetLastError());
+    std::vector<double> st((size_t)nrow * 9);
+    TMX_CK(cudaMemcpyAsync(st.data(), h->stats, st.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    TMX_CK(cudaStreamSynchronize(h->stream));
+    // running maxima over the rows in the reference's order, starting at 0
+    double mx[3] = {0.0, 0.0, 0.0};
+    for (int r = 0; r < nrow; r++) {
+        const double* s = &st[(size_t)r * 9];
+        double* o = rows_out + (size_t)r * 7;
+        const bool mixing_row = r < G.mny;
+        o[0] = mixing_row ? r + 1 : (r - G.mny + 1) + G.mny;
+        for (int q = 0; q < 3; q++) {
+            if (mx[q] < s[6 + q]) mx[q] = s[6 + q];
+            o[1 + q] = s[q];
+        }
+        const bool ok = mixing_row ? (s[0] > 0 && s[1] > 0 && s[2] > 0) : (s[0] > 0);
+        for (int q = 0; q < 3; q++) {
+            if (ok) {
+                const double Is = s[3 + q] / (s[q] * (mx[q] - s[q]));
+                o[4 + q] = 1.0 - std::sqrt(Is);
+            } else {
+                o[4 + q] = 0.0;
+            }
+        }
+    }
+    if (outlet_im)
+        for (int q = 0; q < 3; q++) outlet_im[q] = rows_out[4 + q];
+    return TMX_OK;
+}
+
+int tmx_sums(tmx_handle* h, double out[8])
+{
+    if (!h || !out) return fail(TMX_E_INVALID, "null argument");
+    if (!h->inited) return fail(TMX_E_STATE, "tmx_sums before tmx_init");
+    TMX_CK(cudaSetDevice(h->device));
+    tmx::k_sums<<<kSumBlocks, 256, 0, h->stream>>>(h->mac, h->G, h->partial);
+    TMX_CK(cudaGetLastError());
+    std::vector<double> p((size_t)kSumBlocks * 6);
+    TMX_CK(cudaMemcpyAsync(p.data(), h->partial, p.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    TMX_CK(cudaStreamSynchronize(h->stream));
+    double s[6] = {0, 0, 0, 0, 0, 0};
+    for (int b = 0; b < kSumBlocks; b++)
+        for (int m = 0; m < 6; m++) s[m] += p[(size_t)b * 6 + m];
+    out[0] = s[0];
+    out[1] = s[1];
+    out[2] = s[2];
+    out[3] = s[3];
+    out[4] = s[1] + s[2] + s[3];
+    out[5] = s[4];
+    out[6] = s[5];
+    out[7] = (double)h->G.nnodes;
+    return TMX_OK;
+}
+
+int tmx_inlet_profile(tmx_handle* h, double* uin1, double* uin2)
+{
+    if (!h || !uin1 || !uin2) return fail(TMX_E_INVALID, "null argument");
+    if (!h->inited) return fail(TMX_E_STATE, "tmx_inlet_profile before tmx_init");
+    std::memcpy(uin1, h->uin1.data(), h->uin1.size() * sizeof(double));
+    std::memcpy(uin2, h->uin2.data(), h->uin2.size() * sizeof(double));
+    return TMX_OK;
+}
+
+int tmx_step_timed(tmx_handle* h, int nsteps, double* ms_bulk, double* ms_boundary, double* ms_total)
+{
+    if (!h) return fail(TMX_E_INVALID, "null handle");
+    if (!h->inited) return fail(TMX_E_STATE, "tmx_step_timed before tmx_init");
+    if (nsteps <= 0) return fail(TMX_E_INVALID, "nsteps must be positive");
+    TMX_CK(cudaSetDevice(h->device));
+    std::vector<cudaEvent_t> ev((size_t)nsteps * 3);
+    for (auto& x : ev) TMX_CK(cudaEventCreate(&x));
+    cudaEvent_t t0, t1;
+    TMX_CK(cudaEventCreate(&t0));
+    TMX_CK(cudaEventCreate(&t1));
+    TMX_CK(cudaEventRecord(t0, h->stream));
+    int rc = TMX_OK;
+    for (int s = 0; s < nsteps && rc == TMX_OK; s++) rc = launch_step(h, s == nsteps - 1, &ev[(size_t)s * 3]);
+    TMX_CK(cudaEventRecord(t1, h->stream));
+    TMX_CK(cudaEventSynchronize(t1));
+    double sb = 0, sbd = 0;
+    for (int s = 0; s < nsteps && rc == TMX_OK; s++) {
+        float a = 0, b = 0;
+        TMX_CK(cudaEventElapsedTime(&a, ev[(size_t)s * 3], ev[(size_t)s * 3 + 1]));
+        TMX_CK(cudaEventElapsedTime(&b, ev[(size_t)s * 3 + 1], ev[(size_t)s * 3 + 2]));
+        sb += a;
+        sbd += b;
+    }
+    float tot = 0;
+    TMX_CK(cudaEventElapsedTime(&tot, t0, t1));
+    for (auto& x : ev) cudaEventDestroy(x);
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    if (rc) return rc;
+    if (ms_bulk) *ms_bulk = sb;
+    if (ms_boundary) *ms_boundary = sbd;
+    if (ms_total) *ms_total = tot;
+    return TMX_OK;
+}
+
+int tmx_counts(const tmx_handle* h, long long out[4])
+{
+    if (!h || !out) return fail(TMX_E_INVALID, "null argument");
+    out[0] = h->G.nnodes;
+    out[1] = h->G.nnodes - h->nb;
+    out[2] = h->nb;
+    out[3] = h->bytes;
+    return TMX_OK;
+}
+
+void tmx_destroy(tmx_handle* h)
+{
+    if (!h) return;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    free_all(h);
+    delete h;
+}
+
+}  // extern "C"

@@ -1,0 +1,153 @@
+// tmx_device.cuh -- geometry, lattice constants and exact FP64 helpers shared
+// by the T-mixer kernels.  sm_100a only; compiled with --fmad=false so that no
+// multiply-add is contracted implicitly (the reference's x86-64 build has no
+// contraction); the only fused operations are the explicit __fma_rn calls of
+// div_c() below.
+#pragma once
+#include <cstdint>
+
+namespace tmx {
+
+// D3Q19 velocity set in the reference's order (Tmixer.cpp:1368-1370).
+__host__ __device__ constexpr int EX(int q)
+{
+    return (q == 1 || q == 7 || q == 10 || q == 11 || q == 14) ? 1
+         : (q == 3 || q == 8 || q == 9 || q == 12 || q == 13) ? -1 : 0;
+}
+__host__ __device__ constexpr int EY(int q)
+{
+    return (q == 2 || q == 7 || q == 8 || q == 15 || q == 18) ? 1
+         : (q == 4 || q == 9 || q == 10 || q == 16 || q == 17) ? -1 : 0;
+}
+__host__ __device__ constexpr int EZ(int q)
+{
+    return (q == 5 || q == 11 || q == 12 || q == 15 || q == 16) ? 1
+         : (q == 6 || q == 13 || q == 14 || q == 17 || q == 18) ? -1 : 0;
+}
+
+// Geometry of one T-mixer: inlet box 0 (inx x iny x nz) and mixing box 1
+// (mnx x mny x nz); node g of box b at 1-based (i,j,k) is
+// base[b] + ((i-1)*ny[b] + (j-1))*nz + (k-1).  Population q of field f lives at
+// P[(f*19 + q)*ps + g] (structure of arrays, ps >= nnodes).
+struct Geom {
+    int inx, iny, nz, mnx, mny, ia, ib;
+    int nx[2], ny[2];
+    int base[2];
+    int nnodes;
+    long long ps;
+};
+
+// Per-solve physics constants, computed on the host in the reference's order.
+struct Phys {
+    double c1[4];  // 1.0 - 1.0/tau_f  (flow, A, B, C)
+    double c2[4];  // 1.0/tau_f
+    double rateconst;
+    double rho_out;
+    double cin[3][2];
+};
+
+__host__ __device__ inline bool is_boundary(const Geom& G, int b, int i, int j, int k)
+{
+    if (k == 1 || k == G.nz) return true;
+    if (b == 0) return i == 1 || i == G.inx || j == G.iny || (j == 1 && (i <= G.ia || i >= G.ib));
+    return i == 1 || i == G.mnx || j == 1;
+}
+
+__host__ __device__ inline int node_index(const Geom& G, int b, int i, int j, int k)
+{
+    return G.base[b] + ((i - 1) * G.ny[b] + (j - 1)) * G.nz + (k - 1);
+}
+
+// Pull source of direction q for node (b,i,j,k): the reference's streaming()
+// (Tmixer.cpp:9039-9347) including the two interface rules (inlet row 1 over
+// the opening takes 2,7,8,15,18 from mixing row mny, :9077-9085; mixing row
+// mny takes 4,9,10,16,17 from inlet row 1, :9230-9237).  -1 for a source
+// outside both boxes (a ghost node; every such value is replaced by a
+// boundary closure).
+__host__ __device__ inline int pull_src(const Geom& G, int b, int i, int j, int k, int q)
+{
+    int si = i - EX(q), sj = j - EY(q), sk = k - EZ(q), sb = b;
+    if (b == 0 && j == 1 && EY(q) == 1 && i >= G.ia && i <= G.ib) {
+        sb = 1;
+        si = i - G.ia + 1 - EX(q);
+        sj = G.mny;
+    } else if (b == 1 && j == G.mny && EY(q) == -1) {
+        sb = 0;
+        si = i + G.ia - 1 - EX(q);
+        sj = 1;
+    }
+    if (si < 1 || si > G.nx[sb] || sj < 1 || sj > G.ny[sb] || sk < 1 || sk > G.nz) return -1;
+    return node_index(G, sb, si, sj, sk);
+}
+
+// x / d for the constants d = 3, 18, 36, correctly rounded, without a
+// division instruction: q0 = RN(x*r) with r = RN(1/d), the exact remainder
+// x - d*q0 (one FMA) and one correction FMA.  For these d, r is within
+// 2^-54 relative of 1/d, so q0 is within one ulp of x/d and the correction
+// returns RN(x/d) (Markstein's theorem; P. Markstein, IBM J. Res. Dev. 34(1),
+// 1990).  Tiny |x| (possible subnormal quotient) takes the division path.
+__device__ __forceinline__ double div_c(double x, double d, double r)
+{
+    if (fabs(x) < 0x1p-1000) return __ddiv_rn(x, d);
+    double q = __dmul_rn(x, r);
+    double e = __fma_rn(-q, d, x);
+    return __fma_rn(e, r, q);
+}
+
+__device__ __forceinline__ double feq_div(double x, int q)
+{
+    if (q == 0) return div_c(x, 3.0, 1.0 / 3.0);
+    if (q <= 6) return div_c(x, 18.0, 1.0 / 18.0);
+    return div_c(x, 36.0, 1.0 / 36.0);
+}
+
+// lattice weights as the reference stores them (Tmixer.cpp:706-709)
+__device__ __forceinline__ double wq(int q) { return q == 0 ? 1.0 / 3.0 : (q <= 6 ? 1.0 / 18.0 : 1.0 / 36.0); }
+
+// e_q . u as the reference sums it, ((ux*ex + uy*ey) + uz*ez).  The products
+// by 0 and +-1 are exact and adding a zero changes at most the sign of a zero
+// result (which the equilibrium polynomial absorbs), so only the sum of the
+// two non-zero terms rounds; q is a compile-time constant after unrolling.
+__device__ __forceinline__ double e_dot_u(int q, double ux, double uy, double uz)
+{
+    const double a = EX(q) > 0 ? ux : -ux, b = EY(q) > 0 ? uy : -uy, c = EZ(q) > 0 ? uz : -uz;
+    if (EX(q) != 0) return EY(q) != 0 ? a + b : (EZ(q) != 0 ? a + c : a);
+    if (EY(q) != 0) return EZ(q) != 0 ? b + c : b;
+    return EZ(q) != 0 ? c : 0.0;
+}
+
+// Equilibrium polynomial shared by the four fields (they use the flow
+// velocity; Tmixer.cpp:1602-1830):
+//   q=0:  1.0 - 3.0*u2/2.0
+//   q>0:  1.0 + 3.0*eu - 3.0*u2/2.0 + 9.0*eu*eu/2.0   (C left-to-right)
+__device__ __forceinline__ void eq_poly(double ux, double uy, double uz, double (&poly)[19])
+{
+    const double u2 = ux * ux + uy * uy + uz * uz;
+    const double t = 3.0 * u2 / 2.0;
+    poly[0] = 1.0 - t;
+#pragma unroll
+    for (int q = 1; q < 19; q++) {
+        const double eu = e_dot_u(q, ux, uy, uz);
+        poly[q] = 1.0 + 3.0 * eu - t + 9.0 * eu * eu / 2.0;
+    }
+}
+
+// rho = f0 + f1 + ... + f18 in index order (Tmixer.cpp:9391-9560)
+__device__ __forceinline__ double sum19(const double (&v)[19])
+{
+    double s = v[0];
+#pragma unroll
+    for (int q = 1; q < 19; q++) s += v[q];
+    return s;
+}
+
+// momentum sums in index order; zero components drop out exactly
+// (Tmixer.cpp:9597-9609)
+__device__ __forceinline__ void momentum(const double (&f)[19], double& sx, double& sy, double& sz)
+{
+    sx = f[1] - f[3] + f[7] - f[8] - f[9] + f[10] + f[11] - f[12] - f[13] + f[14];
+    sy = f[2] - f[4] + f[7] + f[8] - f[9] - f[10] + f[15] - f[16] - f[17] + f[18];
+    sz = f[5] - f[6] + f[11] + f[12] - f[13] - f[14] + f[15] + f[16] - f[17] - f[18];
+}
+
+}  // namespace tmx
