@@ -1,0 +1,349 @@
+#!/usr/bin/env python
+"""Benchmark of the T-mixer step on B200 (one JSON line on stdout).
+
+Workload (N=1): the single-mixer configuration of the benchmark set, a T-mixer
+of width W=32 (inlet 256x32x32, mixing 64x128x32: 524,288 fluid nodes), flow
+tau 0.56, species tau 0.6, k = 1e-3, inlet profile maximum 0.05, outlet and
+initial density 1, in the plain FP64 form (bit-exact with the reference).
+A "step" is one full lattice-Boltzmann time step of the mixer (flow + 3
+species, all nodes); MLUPS counts node updates of all four fields.
+
+  value      MLUPS over all GPUs: N x nodes x K / (max over ranks of the device
+             time of K steps), CUDA events on the solver's stream, inputs
+             resident in HBM (the 319 MB population set exceeds the 126 MB L2,
+             so no flush is needed between steps).
+  e2e        the whole configured solve (create, init with the host inlet
+             profile, 20,000 steps with the outlet mixing index read back every
+             100 steps, all fields copied to host) through the public API.
+  roofline   the bulk (interior) kernel: 1216 algorithmic bytes per node
+             update (76 FP64 populations read and written) over its average
+             launch time, against the measured HBM copy bandwidth.
+  cpu_baseline  the reference's own OpenMP build (oracle/_ref) on this host's
+             cores, on a bounded number of steps of the same workload.
+
+Multi-GPU (torchrun): every rank solves its own mixer (replicas, no data-path
+collective); the job's value is the sum.  ``--impl reference`` times the
+reference's CPU build instead (rank 0 only).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "MLUPS & %HBM roofline, served FP16-storage vs plain FP64; p50/p99 solve latency"
+UNIT = "MLUPS"
+WORKLOAD = dict(W=32, u_max=0.05, tau_f=0.56, tau_c=0.6, k=1e-3, rho=1.0, steps=20000)
+BYTES_PER_LUP_FP64 = 4 * 19 * 8 * 2
+FALLBACK_HBM_GBS = 6650.0
+
+
+def measured_peaks() -> dict:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            d = json.load(fh)
+        return dict(hbm_gbs=float(d["hbm_gbs"]), source="measured")
+    return dict(hbm_gbs=FALLBACK_HBM_GBS, source="fallback")
+
+
+def workload_spec():
+    import tmixer_b200 as T
+
+    w = WORKLOAD
+    return T.w_layout(w["W"], w["u_max"], w["tau_f"], w["tau_c"], w["k"], w["rho"], steps=w["steps"])
+
+
+def workload_ref_params(spec) -> dict:
+    return dict(inx=spec.inx, iny=spec.iny, nz=spec.nz, mnx=spec.mnx, mny=spec.mny, tau=spec.tau,
+                tau_c=spec.tau_a, umean=spec.umean, rateconst=spec.rateconst, rho0=spec.rho0,
+                rho_out=spec.rho_out, ca_in1=spec.c_in[0][0], ca_in2=spec.c_in[0][1], cb_in1=spec.c_in[1][0],
+                cb_in2=spec.c_in[1][1], cp_in1=spec.c_in[2][0], cp_in2=spec.c_in[2][1])
+
+
+def config_dict(spec, form: str, n_gpus: int) -> dict:
+    return {"workload": "single T-mixer W=%d (inlet %dx%dx%d + mixing %dx%dx%d, %d fluid nodes), %s"
+                        % (WORKLOAD["W"], spec.inx, spec.iny, spec.nz, spec.mnx, spec.mny, spec.nz, spec.nodes(),
+                           form),
+            "form": form, "fluid_nodes": spec.nodes(), "bbox_nodes": spec.inx * (spec.iny + spec.mny) * spec.nz,
+            "tau_f": spec.tau, "tau_c": spec.tau_a, "k": spec.rateconst, "u_max": WORKLOAD["u_max"],
+            "solve_steps": WORKLOAD["steps"], "parallelism": "replicas x%d" % n_gpus,
+            "l2": "state (2 x 319 MB) larger than L2, no flush"}
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (one process per GPU; replicas)
+# ---------------------------------------------------------------------------
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = False
+
+    def init(self, backend: str) -> None:
+        if self.world > 1:
+            import datetime
+
+            import torch.distributed as dist
+
+            dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=120))
+            self.pg = True
+
+    def barrier(self) -> None:
+        if self.pg:
+            import torch.distributed as dist
+
+            dist.barrier()
+
+    def max(self, x: float, device=None) -> float:
+        if not self.pg:
+            return x
+        import torch
+        import torch.distributed as dist
+
+        t = torch.tensor([x], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self) -> None:
+        if self.pg:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+            self.pg = False
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self) -> None:
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.QUERY,
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict | None:
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as fh:
+            for line in fh:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    mx.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for nm, v in zip(names, parts[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# the reference's CPU build (oracle/_ref), used as cpu_baseline and as the
+# reference arm.  The oracle package is test infrastructure; only this
+# baseline leg runs it.
+# ---------------------------------------------------------------------------
+def reference_cpu_run(spec, budget_s: float, max_steps: int | None = None) -> dict:
+    from oracle import build_ref, oracle as O
+
+    params = workload_ref_params(spec)
+    binary = build_ref.binary_path("bench_w%d" % WORKLOAD["W"], params)
+    cores = os.cpu_count() or 1
+    if not os.path.exists(binary):
+        if os.path.exists(build_ref.REF_SRC):
+            binary = build_ref.build("bench_w%d" % WORKLOAD["W"], params)
+        else:
+            return {"error": "reference binary for this workload not built"}
+    # probe: 1 warm-up + 2 timed steps to size the sample
+    _, _, t2 = O.run_ref(binary, 3, threads=cores, warmup=1)
+    per = max(t2 / 2.0, 1e-4)
+    n = int(max(3, min(budget_s / per, 400)))
+    if max_steps is not None:
+        n = max(1, min(n, max_steps))
+    _, _, secs = O.run_ref(binary, n + 1, threads=cores, warmup=1)
+    value = spec.nodes() * n / secs / 1e6
+    return {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": "%d timed steps (after 1 warm-up) of the same W=%d mixer, reference OpenMP build "
+                      "(g++ -O2 -fopenmp), OMP_NUM_THREADS=%d; %.2f s" % (n, WORKLOAD["W"], cores, secs),
+            "seconds": secs, "steps": n}
+
+
+def profile_traffic() -> dict | None:
+    """DRAM bytes per launch of the bulk kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "k_bulk_fp64_w32.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as fh:
+        return json.load(fh)
+
+
+# ---------------------------------------------------------------------------
+def run_ours(args, dist: Dist) -> dict | None:
+    import torch
+
+    import tmixer_b200 as T
+
+    torch.cuda.set_device(dist.local_rank)
+    dist.init("nccl")
+    dev = torch.device("cuda", dist.local_rank)
+    spec = workload_spec()
+    nodes = spec.nodes()
+    peaks = measured_peaks()
+
+    s = T.Solver(spec, device=dist.local_rank).init()
+    s.step(args.warmup)
+    s.sync()
+    counts = s.counts()
+
+    # --- value: K steps, events on the solver's stream, max over ranks ----
+    clocks = ClockSampler(dist.local_rank)
+    torch.cuda.synchronize()
+    dist.barrier()
+    clocks.start()
+    ms = s.time_steps(args.steps)
+    torch.cuda.synchronize()
+    dist.barrier()
+    clk = clocks.stop()
+    ms_max = dist.max(ms, dev)
+    value = dist.world * nodes * args.steps / (ms_max * 1e-3) / 1e6
+
+    # --- roofline of the dominant kernel: per-launch events --------------
+    kr = min(args.steps, 400)
+    tb, tbd, tt = s.step_timed(kr)
+    bulk_ms = tb / kr
+    bnd_ms = tbd / kr
+    bulk_bytes = counts["interior"] * BYTES_PER_LUP_FP64
+    achieved = bulk_bytes / (bulk_ms * 1e-3) / 1e9
+    prof = profile_traffic()
+    traffic = None
+    if prof and prof.get("nodes") == nodes:
+        traffic = prof.get("dram_bytes_per_launch")
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
+                "kernel": "k_bulk (interior nodes, %d per launch)" % counts["interior"],
+                "peak_source": peaks["source"],
+                "algorithmic_bytes_per_launch": bulk_bytes,
+                "boundary_kernel_ms": bnd_ms, "bulk_kernel_ms": bulk_ms,
+                "step_effective_gbs": nodes * BYTES_PER_LUP_FP64 / (ms_max / args.steps * 1e-3) / 1e9}
+    s.close()
+
+    # --- e2e: the configured solve through the public API ---------------
+    e2e_steps = args.e2e_steps
+    dist.barrier()
+    t0 = time.perf_counter()
+    s2 = T.Solver(spec, device=dist.local_rank)
+    s2.init()
+    done = 0
+    im_reads = 0
+    while done < e2e_steps:
+        c = min(100, e2e_steps - done)
+        s2.step(c)
+        done += c
+        s2.mixing()  # outlet mixing index read back (D2H) every 100 steps
+        im_reads += 1
+    outs = [s2.field(b, f) for b in (0, 1) for f in T.FIELDS]
+    s2.close()
+    t1 = time.perf_counter()
+    e2e_s = dist.max(t1 - t0, dev)
+    h2d = 2 * (spec.iny + 3) * (spec.nz + 3) * 8 + counts["boundary"] * 5
+    d2h = sum(o.nbytes for o in outs) + im_reads * (spec.mny + spec.iny) * 9 * 8
+    e2e = {"value": dist.world * nodes * e2e_steps / e2e_s / 1e6, "unit": UNIT,
+           "h2d_bytes_per_step": h2d / e2e_steps, "d2h_bytes_per_step": d2h / e2e_steps,
+           "steps": e2e_steps, "seconds": e2e_s,
+           "what": "create + init + %d steps + mixing index every 100 steps + all fields to host" % e2e_steps}
+
+    cpu = None
+    if dist.world == 1 and dist.rank == 0 and not args.no_cpu_baseline:
+        cpu = reference_cpu_run(spec, budget_s=args.cpu_budget)
+    dist.close()
+    if dist.rank != 0:
+        return None
+    return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config_dict(spec, "plain FP64 (bit-exact with the reference)", dist.world),
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+            "gpu_launches": 2 * args.steps}
+
+
+def run_reference(args, dist: Dist) -> dict | None:
+    if dist.rank != 0:
+        return None
+    spec = workload_spec()
+    budget = args.cpu_budget * 2
+    r = reference_cpu_run(spec, budget_s=budget, max_steps=args.steps)
+    if "error" in r:
+        return {"impl": "reference", "unavailable": r["error"]}
+    return {"impl": "reference", "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": dist.world,
+            "steps": r["steps"], "warmup": 1, "ms_per_step": r["seconds"] / r["steps"] * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config_dict(spec, "reference OpenMP CPU build", dist.world),
+            "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": "reference",
+                             "sample": r["sample"]},
+            "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--e2e-steps", type=int, default=WORKLOAD["steps"])
+    ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of reference CPU steps")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args(argv)
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    dist = Dist()
+    if dist.world != args.gpus and "WORLD_SIZE" in os.environ:
+        print("warning: --gpus %d but WORLD_SIZE %d" % (args.gpus, dist.world), file=sys.stderr)
+    out = run_reference(args, dist) if args.impl == "reference" else run_ours(args, dist)
+    if out is not None:
+        print(json.dumps(out))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

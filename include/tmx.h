@@ -155,6 +155,11 @@ int tmx_inlet_profile(tmx_handle *h, double *uin1, double *uin2);
  * Benchmark support; no counterpart in the reference. */
 int tmx_step_timed(tmx_handle *h, int nsteps, double *ms_bulk, double *ms_boundary, double *ms_total);
 
+/* Run nsteps steps exactly as tmx_step does, between two CUDA events recorded
+ * on the handle's stream, wait for them, and return the elapsed device time
+ * (ms).  Benchmark support; no counterpart in the reference. */
+int tmx_time_steps(tmx_handle *h, int nsteps, double *ms);
+
 /* Node counts: out[0] fluid nodes (both boxes), out[1] interior nodes,
  * out[2] boundary nodes, out[3] device bytes allocated. */
 int tmx_counts(const tmx_handle *h, long long out[4]);

@@ -98,7 +98,13 @@ def patched_source(params: dict) -> str:
 
 
 def binary_path(name: str, params: dict) -> str:
+    """Binary name: case parameters plus the harness and this recipe, so a
+    changed harness or patch list never reuses a stale binary."""
     key = json.dumps({k: params[k] for k in sorted(params)}, sort_keys=True)
+    with open(HARNESS, "rb") as fh:
+        key += hashlib.sha1(fh.read()).hexdigest()
+    with open(os.path.abspath(__file__), "rb") as fh:
+        key += hashlib.sha1(fh.read()).hexdigest()
     h = hashlib.sha1(key.encode()).hexdigest()[:10]
     return os.path.join(OUT_DIR, "tmixer_ref_%s_%s" % (name, h))
 

@@ -173,13 +173,16 @@ def read_ref_mixing(path: str) -> np.ndarray:
     return np.array(rows, dtype=np.float64)
 
 
-def run_ref(binary: str, steps: int, with_pops: bool = False, threads: int | None = None):
-    """Run a reference binary in a scratch directory; return (dump, mixing rows, seconds)."""
+def run_ref(binary: str, steps: int, with_pops: bool = False, threads: int | None = None, warmup: int = 0):
+    """Run a reference binary in a scratch directory; return (dump, mixing
+    rows, seconds of the timed loop: the steps after the first ``warmup``)."""
     env = dict(os.environ)
     if threads:
         env["OMP_NUM_THREADS"] = str(threads)
     with tempfile.TemporaryDirectory() as d:
         args = [binary, str(steps), os.path.join(d, "out.bin")] + (["pops"] if with_pops else [])
+        if warmup:
+            args.append("warmup=%d" % warmup)
         r = subprocess.run(args, cwd=d, env=env, capture_output=True, text=True, check=True)
         secs = None
         for line in r.stderr.splitlines():

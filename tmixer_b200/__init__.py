@@ -81,6 +81,7 @@ def lib() -> ctypes.CDLL:
     L.tmx_inlet_profile.argtypes = [vp, vp, vp]
     L.tmx_step_timed.argtypes = [vp, ip, P(dp), P(dp), P(dp)]
     L.tmx_counts.argtypes = [vp, P(ctypes.c_longlong)]
+    L.tmx_time_steps.argtypes = [vp, ip, P(dp)]
     L.tmx_destroy.argtypes = [vp]
     L.tmx_destroy.restype = None
     if L.tmx_abi_version() != ABI_VERSION:
@@ -265,6 +266,13 @@ class Solver:
         a, b, t = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
         _check(lib().tmx_step_timed(self._h, int(n), ctypes.byref(a), ctypes.byref(b), ctypes.byref(t)))
         return a.value, b.value, t.value
+
+    def time_steps(self, n: int) -> float:
+        """Run n steps (the ``step`` path) between CUDA events on the solver's
+        stream; returns the device time in ms."""
+        ms = ctypes.c_double()
+        _check(lib().tmx_time_steps(self._h, int(n), ctypes.byref(ms)))
+        return ms.value
 
     def counts(self) -> dict:
         o = (ctypes.c_longlong * 4)()

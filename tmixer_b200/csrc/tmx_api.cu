@@ -68,6 +68,12 @@ struct tmx_handle {
     bool inited = false;
     long long bytes = 0;
     int bulk_blocks = 0;
+    // the boundary kernel runs on a second stream, concurrently with the bulk
+    // kernel (disjoint outputs, read-only shared inputs)
+    cudaStream_t aux = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+    // one captured step per (state buffer, macroscopic output) combination
+    cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
 };
 
 namespace {
@@ -230,6 +236,17 @@ void free_all(tmx_handle* h)
         cudaFree(h->uin_d[s]);
         h->pop[s] = h->rho[s] = h->uin_d[s] = nullptr;
     }
+    for (int a = 0; a < 2; a++)
+        for (int m = 0; m < 2; m++)
+            if (h->graph[a][m]) {
+                cudaGraphExecDestroy(h->graph[a][m]);
+                h->graph[a][m] = nullptr;
+            }
+    if (h->fork) cudaEventDestroy(h->fork);
+    if (h->join) cudaEventDestroy(h->join);
+    h->fork = h->join = nullptr;
+    if (h->aux) cudaStreamDestroy(h->aux);
+    h->aux = nullptr;
     cudaFree(h->mac);
     cudaFree(h->bnode);
     cudaFree(h->bcls);
@@ -242,26 +259,71 @@ void free_all(tmx_handle* h)
     h->stream = nullptr;
 }
 
-int launch_step(tmx_handle* h, int write_macro, cudaEvent_t* ev /* 3 events or null */)
+// Queue the two kernels of one step from buffer `cur`: the boundary kernel on
+// the auxiliary stream, forked from and joined back into the main stream, and
+// the bulk kernel on the main stream.  With ev (4 events) each kernel is
+// bracketed by its own pair of events.  The state and density buffers flip
+// together every step, so one parity index selects both.
+int enqueue_step(tmx_handle* h, int cur, int write_macro, cudaEvent_t* ev)
 {
     const Geom& G = h->G;
-    const double* pin = h->pop[h->cur];
-    double* pout = h->pop[1 - h->cur];
-    const double* rprev = h->rho[h->rcur];
-    double* rcur = h->rho[1 - h->rcur];
+    const double* pin = h->pop[cur];
+    double* pout = h->pop[1 - cur];
+    const double* rprev = h->rho[cur];
+    double* rcur = h->rho[1 - cur];
+    TMX_CK(cudaEventRecord(h->fork, h->stream));
+    TMX_CK(cudaStreamWaitEvent(h->aux, h->fork, 0));
+    if (ev) TMX_CK(cudaEventRecord(ev[2], h->aux));
+    if (h->nb > 0)
+        tmx::k_boundary<<<(h->nb + 127) / 128, 128, 0, h->aux>>>(pin, pout, rprev, rcur, h->mac, h->bnode, h->bcls,
+                                                                h->nb, h->uin_d[0], h->uin_d[1], G, h->P,
+                                                                write_macro);
+    if (ev) TMX_CK(cudaEventRecord(ev[3], h->aux));
+    TMX_CK(cudaEventRecord(h->join, h->aux));
     if (ev) TMX_CK(cudaEventRecord(ev[0], h->stream));
     tmx::k_bulk<<<h->bulk_blocks, 256, 0, h->stream>>>(pin, pout, rcur, h->mac, G, h->P, write_macro);
     if (ev) TMX_CK(cudaEventRecord(ev[1], h->stream));
-    if (h->nb > 0)
-        tmx::k_boundary<<<(h->nb + 127) / 128, 128, 0, h->stream>>>(pin, pout, rprev, rcur, h->mac, h->bnode, h->bcls,
-                                                                   h->nb, h->uin_d[0], h->uin_d[1], G, h->P,
-                                                                   write_macro);
-    if (ev) TMX_CK(cudaEventRecord(ev[2], h->stream));
+    TMX_CK(cudaStreamWaitEvent(h->stream, h->join, 0));
     TMX_CK(cudaGetLastError());
+    return TMX_OK;
+}
+
+int advance(tmx_handle* h)
+{
     h->cur = 1 - h->cur;
-    h->rcur = 1 - h->rcur;
+    h->rcur = h->cur;
     h->steps++;
     return TMX_OK;
+}
+
+// One step through a captured graph (built on first use for this parity and
+// output flag).
+int graph_step(tmx_handle* h, int write_macro)
+{
+    cudaGraphExec_t& ex = h->graph[h->cur][write_macro];
+    if (!ex) {
+        cudaGraph_t gr = nullptr;
+        TMX_CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+        int rc = enqueue_step(h, h->cur, write_macro, nullptr);
+        cudaError_t e = cudaStreamEndCapture(h->stream, &gr);
+        if (rc) {
+            if (gr) cudaGraphDestroy(gr);
+            return rc;
+        }
+        TMX_CK(e);
+        e = cudaGraphInstantiate(&ex, gr, 0);
+        cudaGraphDestroy(gr);
+        TMX_CK(e);
+    }
+    TMX_CK(cudaGraphLaunch(ex, h->stream));
+    return advance(h);
+}
+
+int timed_step(tmx_handle* h, int write_macro, cudaEvent_t* ev)
+{
+    int rc = enqueue_step(h, h->cur, write_macro, ev);
+    if (rc) return rc;
+    return advance(h);
 }
 
 }  // namespace
@@ -409,6 +471,9 @@ int tmx_create(const tmx_case* c, int device, tmx_handle** out)
         return e;
     };
     cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->aux, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->join, cudaEventDisableTiming);
     for (int s = 0; s < 2 && e == cudaSuccess; s++) {
         e = alloc((void**)&h->pop[s], (size_t)76 * G.ps * sizeof(double));
         if (e == cudaSuccess) e = alloc((void**)&h->rho[s], (size_t)4 * G.ps * sizeof(double));
@@ -461,7 +526,7 @@ int tmx_step(tmx_handle* h, int nsteps)
     if (nsteps < 0) return fail(TMX_E_INVALID, "negative step count");
     TMX_CK(cudaSetDevice(h->device));
     for (int s = 0; s < nsteps; s++) {
-        int rc = launch_step(h, s == nsteps - 1, nullptr);
+        int rc = graph_step(h, s == nsteps - 1);
         if (rc) return rc;
     }
     return TMX_OK;
@@ -477,18 +542,32 @@ int tmx_sync(tmx_handle* h)
 
 long long tmx_steps_done(const tmx_handle* h) { return h ? h->steps : -1; }
 
+// Copy n = nx*ny*nz doubles of one box from the device (x fastest) into host
+// memory in the reference's [i][j][k] order (k fastest).
+static int box_to_host(tmx_handle* h, int box, const double* dev, double* host_out, std::vector<double>& stage)
+{
+    const Geom& G = h->G;
+    const int nx = G.nx[box], ny = G.ny[box], nz = G.nz;
+    const size_t n = (size_t)nx * ny * nz;
+    stage.resize(n);
+    TMX_CK(cudaMemcpyAsync(stage.data(), dev + G.base[box], n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    TMX_CK(cudaStreamSynchronize(h->stream));
+    for (int k = 0; k < nz; k++)
+        for (int j = 0; j < ny; j++) {
+            const double* src = stage.data() + ((size_t)k * ny + j) * nx;
+            for (int i = 0; i < nx; i++) host_out[((size_t)i * ny + j) * nz + k] = src[i];
+        }
+    return TMX_OK;
+}
+
 int tmx_fields(tmx_handle* h, int box, int field, double* host_out)
 {
     if (!h || !host_out) return fail(TMX_E_INVALID, "null argument");
     if (box < 0 || box > 1 || field < 0 || field > 6) return fail(TMX_E_INVALID, "box %d / field %d out of range", box, field);
     if (!h->inited) return fail(TMX_E_STATE, "tmx_fields before tmx_init");
     TMX_CK(cudaSetDevice(h->device));
-    const Geom& G = h->G;
-    const size_t n = (size_t)G.nx[box] * G.ny[box] * G.nz;
-    TMX_CK(cudaMemcpyAsync(host_out, h->mac + (size_t)field * G.ps + G.base[box], n * sizeof(double),
-                           cudaMemcpyDeviceToHost, h->stream));
-    TMX_CK(cudaStreamSynchronize(h->stream));
-    return TMX_OK;
+    std::vector<double> stage;
+    return box_to_host(h, box, h->mac + (size_t)field * h->G.ps, host_out, stage);
 }
 
 int tmx_populations(tmx_handle* h, int box, int fld, double* host_out)
@@ -499,10 +578,11 @@ int tmx_populations(tmx_handle* h, int box, int fld, double* host_out)
     TMX_CK(cudaSetDevice(h->device));
     const Geom& G = h->G;
     const size_t n = (size_t)G.nx[box] * G.ny[box] * G.nz;
-    for (int q = 0; q < 19; q++)
-        TMX_CK(cudaMemcpyAsync(host_out + q * n, h->pop[h->cur] + (size_t)(fld * 19 + q) * G.ps + G.base[box],
-                               n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-    TMX_CK(cudaStreamSynchronize(h->stream));
+    std::vector<double> stage;
+    for (int q = 0; q < 19; q++) {
+        int rc = box_to_host(h, box, h->pop[h->cur] + (size_t)(fld * 19 + q) * G.ps, host_out + q * n, stage);
+        if (rc) return rc;
+    }
     return TMX_OK;
 }
 
@@ -583,21 +663,21 @@ int tmx_step_timed(tmx_handle* h, int nsteps, double* ms_bulk, double* ms_bounda
     if (!h->inited) return fail(TMX_E_STATE, "tmx_step_timed before tmx_init");
     if (nsteps <= 0) return fail(TMX_E_INVALID, "nsteps must be positive");
     TMX_CK(cudaSetDevice(h->device));
-    std::vector<cudaEvent_t> ev((size_t)nsteps * 3);
+    std::vector<cudaEvent_t> ev((size_t)nsteps * 4);
     for (auto& x : ev) TMX_CK(cudaEventCreate(&x));
     cudaEvent_t t0, t1;
     TMX_CK(cudaEventCreate(&t0));
     TMX_CK(cudaEventCreate(&t1));
     TMX_CK(cudaEventRecord(t0, h->stream));
     int rc = TMX_OK;
-    for (int s = 0; s < nsteps && rc == TMX_OK; s++) rc = launch_step(h, s == nsteps - 1, &ev[(size_t)s * 3]);
+    for (int s = 0; s < nsteps && rc == TMX_OK; s++) rc = timed_step(h, s == nsteps - 1, &ev[(size_t)s * 4]);
     TMX_CK(cudaEventRecord(t1, h->stream));
     TMX_CK(cudaEventSynchronize(t1));
     double sb = 0, sbd = 0;
     for (int s = 0; s < nsteps && rc == TMX_OK; s++) {
         float a = 0, b = 0;
-        TMX_CK(cudaEventElapsedTime(&a, ev[(size_t)s * 3], ev[(size_t)s * 3 + 1]));
-        TMX_CK(cudaEventElapsedTime(&b, ev[(size_t)s * 3 + 1], ev[(size_t)s * 3 + 2]));
+        TMX_CK(cudaEventElapsedTime(&a, ev[(size_t)s * 4], ev[(size_t)s * 4 + 1]));
+        TMX_CK(cudaEventElapsedTime(&b, ev[(size_t)s * 4 + 2], ev[(size_t)s * 4 + 3]));
         sb += a;
         sbd += b;
     }
@@ -610,6 +690,28 @@ int tmx_step_timed(tmx_handle* h, int nsteps, double* ms_bulk, double* ms_bounda
     if (ms_bulk) *ms_bulk = sb;
     if (ms_boundary) *ms_boundary = sbd;
     if (ms_total) *ms_total = tot;
+    return TMX_OK;
+}
+
+int tmx_time_steps(tmx_handle* h, int nsteps, double* ms)
+{
+    if (!h || !ms) return fail(TMX_E_INVALID, "null argument");
+    if (!h->inited) return fail(TMX_E_STATE, "tmx_time_steps before tmx_init");
+    if (nsteps <= 0) return fail(TMX_E_INVALID, "nsteps must be positive");
+    TMX_CK(cudaSetDevice(h->device));
+    cudaEvent_t t0, t1;
+    TMX_CK(cudaEventCreate(&t0));
+    TMX_CK(cudaEventCreate(&t1));
+    TMX_CK(cudaEventRecord(t0, h->stream));
+    int rc = tmx_step(h, nsteps);
+    TMX_CK(cudaEventRecord(t1, h->stream));
+    TMX_CK(cudaEventSynchronize(t1));
+    float el = 0;
+    TMX_CK(cudaEventElapsedTime(&el, t0, t1));
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    if (rc) return rc;
+    *ms = el;
     return TMX_OK;
 }
 

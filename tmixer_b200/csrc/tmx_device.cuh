@@ -27,8 +27,10 @@ __host__ __device__ constexpr int EZ(int q)
 
 // Geometry of one T-mixer: inlet box 0 (inx x iny x nz) and mixing box 1
 // (mnx x mny x nz); node g of box b at 1-based (i,j,k) is
-// base[b] + ((i-1)*ny[b] + (j-1))*nz + (k-1).  Population q of field f lives at
-// P[(f*19 + q)*ps + g] (structure of arrays, ps >= nnodes).
+// base[b] + ((k-1)*ny[b] + (j-1))*nx[b] + (i-1): x is the contiguous axis, so
+// the z and y walls (three quarters of all boundary nodes) are contiguous rows.
+// Population q of field f lives at P[(f*19 + q)*ps + g] (structure of arrays,
+// ps >= nnodes, a multiple of 64).
 struct Geom {
     int inx, iny, nz, mnx, mny, ia, ib;
     int nx[2], ny[2];
@@ -55,7 +57,19 @@ __host__ __device__ inline bool is_boundary(const Geom& G, int b, int i, int j, 
 
 __host__ __device__ inline int node_index(const Geom& G, int b, int i, int j, int k)
 {
-    return G.base[b] + ((i - 1) * G.ny[b] + (j - 1)) * G.nz + (k - 1);
+    return G.base[b] + ((k - 1) * G.ny[b] + (j - 1)) * G.nx[b] + (i - 1);
+}
+
+// box and 1-based coordinates of node g
+__host__ __device__ inline void decode(const Geom& G, int g, int& b, int& i, int& j, int& k)
+{
+    b = g >= G.base[1];
+    const int l = g - G.base[b];
+    const int nx = G.nx[b], ny = G.ny[b];
+    i = l % nx + 1;
+    const int t = l / nx;
+    j = t % ny + 1;
+    k = t / ny + 1;
 }
 
 // Pull source of direction q for node (b,i,j,k): the reference's streaming()
@@ -85,12 +99,12 @@ __host__ __device__ inline int pull_src(const Geom& G, int b, int i, int j, int 
 // x - d*q0 (one FMA) and one correction FMA.  For these d, r is within
 // 2^-54 relative of 1/d, so q0 is within one ulp of x/d and the correction
 // returns RN(x/d) (Markstein's theorem; P. Markstein, IBM J. Res. Dev. 34(1),
-// 1990).  Tiny |x| (possible subnormal quotient) takes the division path.
+// 1990).  Valid for x = 0 and for |x| >= 2^-1000 (no subnormal intermediate);
+// callers route tinier operands to feq_div_exact().
 __device__ __forceinline__ double div_c(double x, double d, double r)
 {
-    if (fabs(x) < 0x1p-1000) return __ddiv_rn(x, d);
-    double q = __dmul_rn(x, r);
-    double e = __fma_rn(-q, d, x);
+    const double q = __dmul_rn(x, r);
+    const double e = __fma_rn(-q, d, x);
     return __fma_rn(e, r, q);
 }
 
@@ -100,6 +114,15 @@ __device__ __forceinline__ double feq_div(double x, int q)
     if (q <= 6) return div_c(x, 18.0, 1.0 / 18.0);
     return div_c(x, 36.0, 1.0 / 36.0);
 }
+
+__device__ __forceinline__ double feq_div_exact(double x, int q)
+{
+    return q == 0 ? __ddiv_rn(x, 3.0) : (q <= 6 ? __ddiv_rn(x, 18.0) : __ddiv_rn(x, 36.0));
+}
+
+// A density for which rho*poly could fall below 2^-1000 (the equilibrium
+// polynomial stays above 1/2 for the lattice velocities a stable run has).
+__device__ __forceinline__ bool tiny_density(double r) { return r != 0.0 && fabs(r) < 0x1p-990; }
 
 // lattice weights as the reference stores them (Tmixer.cpp:706-709)
 __device__ __forceinline__ double wq(int q) { return q == 0 ? 1.0 / 3.0 : (q <= 6 ? 1.0 / 18.0 : 1.0 / 36.0); }

@@ -29,34 +29,39 @@
 namespace tmx {
 
 // ---------------------------------------------------------------------------
-// shared per-node physics: moments -> equilibrium -> collision -> store
+// shared per-node physics: equilibrium -> collision -> store
 // ---------------------------------------------------------------------------
 
 // Collide one field given its populations f, density r and the shared
-// equilibrium polynomial, and store the result.  sgn/rt implement the
-// reaction source of Tmixer.cpp:9697-9761: species A and B lose w_q*rt*1.0,
-// C gains w_q*rt*2.0 (molecular weights Ma = Mb = 1, Mp = 2, :9667).
-template <int FLD>
-__device__ __forceinline__ void collide_store(double* __restrict__ Pout, long long ps, int g, const double (&f)[19],
-                                              double r, const double (&poly)[19], const Phys& P, double rt)
+// equilibrium polynomial, and store the result.  The reaction source of
+// Tmixer.cpp:9697-9761: species A and B (fld 1, 2) lose (w_q*rt)*1.0, C gains
+// (w_q*rt)*2.0 (molecular weights Ma = Mb = 1, Mp = 2, :9667).  fld may be a
+// run-time value; the arithmetic is the same either way.
+__device__ __forceinline__ void collide_store(double* __restrict__ Pout, long long ps, int g, int fld,
+                                              const double (&f)[19], double r, const double (&poly)[19],
+                                              const Phys& P, double rt)
 {
-    const double c1 = P.c1[FLD], c2 = P.c2[FLD];
+    const double c1 = P.c1[fld], c2 = P.c2[fld];
+    double* out = Pout + (long long)fld * 19 * ps + g;
+    if (!tiny_density(r)) {
 #pragma unroll
-    for (int q = 0; q < 19; q++) {
-        const double feq = feq_div(r * poly[q], q);
-        double v = f[q] * c1 + c2 * feq;
-        if (FLD == 1 || FLD == 2) v = v - wq(q) * rt;
-        if (FLD == 3) v = v + (wq(q) * rt) * 2.0;
-        Pout[(long long)(FLD * 19 + q) * ps + g] = v;
+        for (int q = 0; q < 19; q++) {
+            const double feq = feq_div(r * poly[q], q);
+            double v = f[q] * c1 + c2 * feq;
+            if (fld == 1 || fld == 2) v = v - wq(q) * rt;
+            if (fld == 3) v = v + (wq(q) * rt) * 2.0;
+            out[(long long)q * ps] = v;
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < 19; q++) {
+            const double feq = feq_div_exact(r * poly[q], q);
+            double v = f[q] * c1 + c2 * feq;
+            if (fld == 1 || fld == 2) v = v - wq(q) * rt;
+            if (fld == 3) v = v + (wq(q) * rt) * 2.0;
+            out[(long long)q * ps] = v;
+        }
     }
-}
-
-__device__ __forceinline__ void load19(const double* __restrict__ P, long long ps, int fld, const int (&src)[19],
-                                       double (&v)[19])
-{
-    const double* base = P + (long long)fld * 19 * ps;
-#pragma unroll
-    for (int q = 0; q < 19; q++) v[q] = src[q] >= 0 ? __ldg(base + (long long)q * ps + src[q]) : 0.0;
 }
 
 // ---------------------------------------------------------------------------
@@ -73,14 +78,14 @@ __global__ void k_init(double* __restrict__ Pout, double* __restrict__ R, double
         double f[19], z[19];
 #pragma unroll
         for (int q = 0; q < 19; q++) {
-            f[q] = feq_div(rho0 * poly[q], q);
-            z[q] = feq_div(0.0 * poly[q], q);
+            f[q] = __ddiv_rn(rho0 * poly[q], q == 0 ? 3.0 : (q <= 6 ? 18.0 : 36.0));
+            z[q] = __ddiv_rn(0.0 * poly[q], q == 0 ? 3.0 : (q <= 6 ? 18.0 : 36.0));
         }
         const double rt = P.rateconst * 0.0 * 0.0;
-        collide_store<0>(Pout, ps, g, f, rho0, poly, P, rt);
-        collide_store<1>(Pout, ps, g, z, 0.0, poly, P, rt);
-        collide_store<2>(Pout, ps, g, z, 0.0, poly, P, rt);
-        collide_store<3>(Pout, ps, g, z, 0.0, poly, P, rt);
+        collide_store(Pout, ps, g, 0, f, rho0, poly, P, rt);
+        collide_store(Pout, ps, g, 1, z, 0.0, poly, P, rt);
+        collide_store(Pout, ps, g, 2, z, 0.0, poly, P, rt);
+        collide_store(Pout, ps, g, 3, z, 0.0, poly, P, rt);
         R[g] = rho0;
         R[ps + g] = 0.0;
         R[2 * ps + g] = 0.0;
@@ -94,60 +99,78 @@ __global__ void k_init(double* __restrict__ Pout, double* __restrict__ R, double
 // ---------------------------------------------------------------------------
 // interior nodes
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_bulk(const double* __restrict__ Pin, double* __restrict__ Pout,
-                                              double* __restrict__ Rcur, double* __restrict__ Mac, Geom G, Phys P,
-                                              int write_macro)
+
+// Upstream node of direction q for an interior node: the lattice neighbour in
+// the same box, or across the opening for the inlet's row 1 (iface 1: ey = +1
+// from mixing row mny) and the mixing box's row mny (iface 2: ey = -1 from
+// inlet row 1).  q is a compile-time constant after unrolling.
+__device__ __forceinline__ int bulk_src(const Geom& G, int g, int i, int k, int sy, int sz, int iface, int q)
+{
+    if (EY(q) == 1 && iface == 1) return G.base[1] + ((k - 1 - EZ(q)) * G.mny + (G.mny - 1)) * G.mnx + (i - G.ia - EX(q));
+    if (EY(q) == -1 && iface == 2) return ((k - 1 - EZ(q)) * G.iny) * G.inx + (i + G.ia - 2 - EX(q));
+    return g - (EX(q) + EY(q) * sy + EZ(q) * sz);
+}
+
+__device__ __forceinline__ void bulk_load(const double* __restrict__ Pin, long long ps, int fld, const Geom& G, int g,
+                                          int i, int k, int sy, int sz, int iface, double (&v)[19])
+{
+    const double* base = Pin + (long long)fld * 19 * ps;
+#pragma unroll
+    for (int q = 0; q < 19; q++) v[q] = __ldg(base + (long long)q * ps + bulk_src(G, g, i, k, sy, sz, iface, q));
+}
+
+__global__ void __launch_bounds__(256, 2) k_bulk(const double* __restrict__ Pin, double* __restrict__ Pout,
+                                                 double* __restrict__ Rcur, double* __restrict__ Mac, Geom G, Phys P,
+                                                 int write_macro)
 {
     const long long ps = G.ps;
     for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < G.nnodes; g += gridDim.x * blockDim.x) {
-        const int b = g >= G.base[1];
-        const int l = g - G.base[b];
-        const int ny = G.ny[b], nz = G.nz;
-        const int k = l % nz + 1;
-        const int t = l / nz;
-        const int j = t % ny + 1;
-        const int i = t / ny + 1;
+        int b, i, j, k;
+        decode(G, g, b, i, j, k);
         if (is_boundary(G, b, i, j, k)) continue;
+        const int sy = G.nx[b], sz = G.nx[b] * G.ny[b];
+        const int iface = (b == 0 && j == 1) ? 1 : ((b == 1 && j == G.mny) ? 2 : 0);
 
-        int src[19];
-        const int sx = ny * nz, sy = nz;
-#pragma unroll
-        for (int q = 0; q < 19; q++) src[q] = g - (EX(q) * sx + EY(q) * sy + EZ(q));
-        if (b == 0 && j == 1) {  // opening: pulls with ey = +1 come from mixing row mny
-#pragma unroll
-            for (int q = 0; q < 19; q++)
-                if (EY(q) == 1) src[q] = node_index(G, 1, i - G.ia + 1 - EX(q), G.mny, k - EZ(q));
-        } else if (b == 1 && j == G.mny) {  // top mixing row: ey = -1 from inlet row 1
-#pragma unroll
-            for (int q = 0; q < 19; q++)
-                if (EY(q) == -1) src[q] = node_index(G, 0, i + G.ia - 1 - EX(q), 1, k - EZ(q));
-        }
-
-        // flow
-        double f[19];
-        load19(Pin, ps, 0, src, f);
-        const double rho = sum19(f);
-        double sxm, sym, szm;
-        momentum(f, sxm, sym, szm);
-        const double ux = sxm / rho, uy = sym / rho, uz = szm / rho;
+        // flow: moments, equilibrium polynomial (shared by all four fields:
+        // they use the flow velocity, Tmixer.cpp:1602-1830), collision
         double poly[19];
-        eq_poly(ux, uy, uz, poly);
-        collide_store<0>(Pout, ps, g, f, rho, poly, P, 0.0);
-
-        // species A and B (the reaction needs both densities first)
-        double a[19], c[19];
-        load19(Pin, ps, 1, src, a);
-        load19(Pin, ps, 2, src, c);
-        const double ca = sum19(a), cb = sum19(c);
+        double rho, ux, uy, uz;
+        {
+            double f[19];
+            bulk_load(Pin, ps, 0, G, g, i, k, sy, sz, iface, f);
+            rho = sum19(f);
+            double sxm, sym, szm;
+            momentum(f, sxm, sym, szm);
+            ux = sxm / rho;
+            uy = sym / rho;
+            uz = szm / rho;
+            eq_poly(ux, uy, uz, poly);
+            collide_store(Pout, ps, g, 0, f, rho, poly, P, 0.0);
+        }
+        // species A and B: the reaction needs both densities before either
+        // collides, so their populations are loaded twice (the second time
+        // from cache) rather than held in registers
+        double ca, cb;
+        {
+            double a[19];
+            bulk_load(Pin, ps, 1, G, g, i, k, sy, sz, iface, a);
+            ca = sum19(a);
+            bulk_load(Pin, ps, 2, G, g, i, k, sy, sz, iface, a);
+            cb = sum19(a);
+        }
         const double rt = P.rateconst * ca * cb;
-        collide_store<1>(Pout, ps, g, a, ca, poly, P, rt);
-        collide_store<2>(Pout, ps, g, c, cb, poly, P, rt);
-        // species C
-        load19(Pin, ps, 3, src, a);
-        const double cc = sum19(a);
-        collide_store<3>(Pout, ps, g, a, cc, poly, P, rt);
-
-        // densities that the junction edges read next step (Tmixer.cpp:8609, :8851)
+        double cc;
+        {
+            double a[19];
+            bulk_load(Pin, ps, 1, G, g, i, k, sy, sz, iface, a);
+            collide_store(Pout, ps, g, 1, a, ca, poly, P, rt);
+            bulk_load(Pin, ps, 2, G, g, i, k, sy, sz, iface, a);
+            collide_store(Pout, ps, g, 2, a, cb, poly, P, rt);
+            bulk_load(Pin, ps, 3, G, g, i, k, sy, sz, iface, a);
+            cc = sum19(a);
+            collide_store(Pout, ps, g, 3, a, cc, poly, P, rt);
+        }
+        // densities the junction edges read next step (Tmixer.cpp:8609, :8851)
         if (b == 0 && j == 2 && (i == G.ia || i == G.ib)) {
             Rcur[g] = rho;
             Rcur[ps + g] = ca;
@@ -283,7 +306,7 @@ __device__ __noinline__ void corner_closure(const BCtx& c, int fld, int n, doubl
 // Apply the closure of class `cls` to field fld of the node in c, on v (the
 // node's pulled populations).  Closures follow the reference case by case;
 // the comments give the reference lines.
-__device__ void closure(const BCtx& c, int cls, int fld, double (&v)[19])
+__device__ __forceinline__ void closure(const BCtx& c, int cls, int fld, double (&v)[19])
 {
     const Geom& G = *c.G;
     const bool flow = fld == 0;
@@ -563,6 +586,32 @@ __device__ void closure(const BCtx& c, int cls, int fld, double (&v)[19])
     }
 }
 
+// The post-closure populations of field fld of the boundary node in c.  A
+// species on a wall face is a zero-gradient copy of an interior node's pulled
+// populations (Tmixer.cpp:2766-4237), so it pulls that node directly.
+__device__ __forceinline__ void closed_pull(const BCtx& c, int cls, int fld, double (&v)[19])
+{
+    if (fld > 0) {
+        int di = 0, dj = 0, dk = 0;
+        switch (cls) {
+        case K_FACE_YT: dj = -1; break;
+        case K_FACE_Y1:
+        case K_OUTLET: dj = 1; break;
+        case K_FACE_MX1: di = 1; break;
+        case K_FACE_MXT: di = -1; break;
+        case K_FACE_ZT: dk = -1; break;
+        case K_FACE_Z1: dk = 1; break;
+        default: break;
+        }
+        if (di | dj | dk) {
+            pull_node(c, fld, c.b, c.i + di, c.j + dj, c.k + dk, v);
+            return;
+        }
+    }
+    pull_node(c, fld, c.b, c.i, c.j, c.k, v);
+    closure(c, cls, fld, v);
+}
+
 // ---------------------------------------------------------------------------
 // boundary nodes
 // ---------------------------------------------------------------------------
@@ -584,45 +633,46 @@ __global__ void __launch_bounds__(128) k_boundary(const double* __restrict__ Pin
     c.P = &P;
     c.ps = G.ps;
     c.g = bnode[t];
-    c.b = c.g >= G.base[1];
-    {
-        const int l = c.g - G.base[c.b];
-        const int ny = G.ny[c.b];
-        c.k = l % G.nz + 1;
-        const int tt = l / G.nz;
-        c.j = tt % ny + 1;
-        c.i = tt / ny + 1;
-    }
+    decode(G, c.g, c.b, c.i, c.j, c.k);
     const int cls = bcls[t];
     const long long ps = G.ps;
     const bool outlet = c.b == 1 && c.j == 1;
 
-    double f[19];
-    pull_node(c, 0, c.b, c.i, c.j, c.k, f);
-    closure(c, cls, 0, f);
-    const double rsum = sum19(f);
-    // the outlet row's density is pinned to rho_out (Tmixer.cpp:9575-9582)
-    const double rho = outlet ? P.rho_out : rsum;
-    double sxm, sym, szm;
-    momentum(f, sxm, sym, szm);
-    const double ux = sxm / rho, uy = sym / rho, uz = szm / rho;
     double poly[19];
-    eq_poly(ux, uy, uz, poly);
-    collide_store<0>(Pout, ps, c.g, f, rho, poly, P, 0.0);
-
-    double a[19], bb[19];
-    pull_node(c, 1, c.b, c.i, c.j, c.k, a);
-    closure(c, cls, 1, a);
-    pull_node(c, 2, c.b, c.i, c.j, c.k, bb);
-    closure(c, cls, 2, bb);
-    const double ca = sum19(a), cb = sum19(bb);
+    double rho, ux, uy, uz;
+    {
+        double f[19];
+        closed_pull(c, cls, 0, f);
+        // the outlet row's density is pinned to rho_out (Tmixer.cpp:9575-9582)
+        rho = outlet ? P.rho_out : sum19(f);
+        double sxm, sym, szm;
+        momentum(f, sxm, sym, szm);
+        ux = sxm / rho;
+        uy = sym / rho;
+        uz = szm / rho;
+        eq_poly(ux, uy, uz, poly);
+        collide_store(Pout, ps, c.g, 0, f, rho, poly, P, 0.0);
+    }
+    // species densities first (the reaction couples A and B), then each
+    // species' closure again and its collision
+    double ca = 0.0, cb = 0.0, cc = 0.0;
+#pragma unroll 1
+    for (int fld = 1; fld <= 2; fld++) {
+        double v[19];
+        closed_pull(c, cls, fld, v);
+        const double s = sum19(v);
+        ca = fld == 1 ? s : ca;
+        cb = fld == 2 ? s : cb;
+    }
     const double rt = P.rateconst * ca * cb;
-    collide_store<1>(Pout, ps, c.g, a, ca, poly, P, rt);
-    collide_store<2>(Pout, ps, c.g, bb, cb, poly, P, rt);
-    pull_node(c, 3, c.b, c.i, c.j, c.k, a);
-    closure(c, cls, 3, a);
-    const double cc = sum19(a);
-    collide_store<3>(Pout, ps, c.g, a, cc, poly, P, rt);
+#pragma unroll 1
+    for (int fld = 1; fld <= 3; fld++) {
+        double v[19];
+        closed_pull(c, cls, fld, v);
+        if (fld == 3) cc = sum19(v);
+        const double cf = fld == 1 ? ca : (fld == 2 ? cb : cc);
+        collide_store(Pout, ps, c.g, fld, v, cf, poly, P, rt);
+    }
 
     Rcur[c.g] = rho;
     Rcur[ps + c.g] = ca;
@@ -654,7 +704,7 @@ __global__ void k_mixing_rows(const double* __restrict__ Mac, Geom G, double* __
     const int j = b == 1 ? row + 1 : row - G.mny + 1;
     const int i0 = b == 1 ? 1 : G.ia, i1 = b == 1 ? G.mnx : G.ib;
     const double* cfield = Mac + (long long)(4 + s) * G.ps;
-    double sumx = 0.0, mx = -1.0 / 0.0;
+    double sumx = 0.0, mx = __longlong_as_double(0xfff0000000000000ULL);  // -inf
     for (int i = i0; i <= i1; i++) {
         double sumz = 0.0;
         for (int k = 1; k <= G.nz; k++) {
@@ -692,12 +742,9 @@ __global__ void k_sums(const double* __restrict__ Mac, Geom G, double* __restric
         acc[1] += a;
         acc[2] += b2;
         acc[3] += c3;
-        const int b = g >= G.base[1];
-        if (b == 1) {
-            const int l = g - G.base[1];
-            const int j = (l / G.nz) % G.mny + 1;
-            if (j == 1) acc[4] += r * Mac[2 * G.ps + g];
-        }
+        int b, i, j, k;
+        decode(G, g, b, i, j, k);
+        if (b == 1 && j == 1) acc[4] += r * Mac[2 * G.ps + g];
         const double uxv = Mac[G.ps + g], uyv = Mac[2 * G.ps + g], uzv = Mac[3 * G.ps + g];
         if (!isfinite(r) || !isfinite(a) || !isfinite(b2) || !isfinite(c3) || !isfinite(uxv) || !isfinite(uyv) ||
             !isfinite(uzv))
