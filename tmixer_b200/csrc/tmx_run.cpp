@@ -1,0 +1,121 @@
+// tmx_run -- C++ host driver over the C ABI: the counterpart of the
+// reference's main() (Tmixer.cpp:10413-10490).  It runs one case on one GPU,
+// reports progress and the outlet mixing index every `--every` steps (the
+// reference writes its files every time_step = 1000 steps, :10476), and writes
+// the final fields as raw little-endian doubles plus the mixing rows as text.
+//
+//   tmx_run [--case reference | --case w --W 32 --umax 0.05 --tauf 0.56 --tauc 0.6 --k 1e-3 --rho 1]
+//           [--steps N] [--every M] [--out DIR] [--device D]
+//
+// Output (with --out): DIR/fields.bin = int32 {inx, iny, nz, mnx, mny, ia, ib,
+// steps} then rho, ux, uy, uz, cA, cB, cC of the inlet box and of the mixing
+// box, each in [i][j][k] order; DIR/mixing.txt = one row per line.
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "tmx.h"
+
+static int die(const char* what)
+{
+    std::fprintf(stderr, "tmx_run: %s: %s\n", what, tmx_last_error());
+    return 1;
+}
+
+int main(int argc, char** argv)
+{
+    std::string kind = "reference", out;
+    int W = 32, device = 0;
+    long long steps = -1, every = 1000;
+    double umax = 0.05, tauf = 0.56, tauc = 0.6, k = 1e-3, rho = 1.0;
+    for (int a = 1; a < argc; a++) {
+        auto next = [&](const char* name) -> const char* {
+            if (a + 1 >= argc) {
+                std::fprintf(stderr, "tmx_run: %s needs a value\n", name);
+                std::exit(2);
+            }
+            return argv[++a];
+        };
+        if (!std::strcmp(argv[a], "--case")) kind = next("--case");
+        else if (!std::strcmp(argv[a], "--W")) W = std::atoi(next("--W"));
+        else if (!std::strcmp(argv[a], "--umax")) umax = std::atof(next("--umax"));
+        else if (!std::strcmp(argv[a], "--tauf")) tauf = std::atof(next("--tauf"));
+        else if (!std::strcmp(argv[a], "--tauc")) tauc = std::atof(next("--tauc"));
+        else if (!std::strcmp(argv[a], "--k")) k = std::atof(next("--k"));
+        else if (!std::strcmp(argv[a], "--rho")) rho = std::atof(next("--rho"));
+        else if (!std::strcmp(argv[a], "--steps")) steps = std::atoll(next("--steps"));
+        else if (!std::strcmp(argv[a], "--every")) every = std::atoll(next("--every"));
+        else if (!std::strcmp(argv[a], "--out")) out = next("--out");
+        else if (!std::strcmp(argv[a], "--device")) device = std::atoi(next("--device"));
+        else {
+            std::fprintf(stderr, "usage: %s [--case reference|w] [--W n] [--steps n] [--every n] [--out dir]\n",
+                         argv[0]);
+            return 2;
+        }
+    }
+    tmx_case c;
+    if (kind == "reference") {
+        if (tmx_case_reference(&c)) return die("case");
+        if (steps < 0) steps = 100001;  // the reference loops itr = 0..time (Tmixer.cpp:10467)
+    } else {
+        if (tmx_case_wlayout(W, umax, tauf, tauc, k, rho, &c)) return die("case");
+        if (steps < 0) steps = 1000;
+    }
+    if (every <= 0) every = steps;
+    tmx_handle* h = nullptr;
+    if (tmx_create(&c, device, &h)) return die("create");
+    const auto t0 = std::chrono::steady_clock::now();
+    if (tmx_init(h)) return die("init");
+    const long long nodes = (long long)c.inx * c.iny * c.nz + (long long)c.mnx * c.mny * c.nz;
+    std::printf("nx:%d ny:%d nz:%d ia:%d ib:%d nodes:%lld steps:%lld\n", c.inx, c.iny + c.mny, c.nz, c.ia,
+                c.ia + c.mnx - 1, nodes, steps);
+    std::vector<double> rows((size_t)(c.mny + c.iny) * 7);
+    double im[3];
+    long long done = 0;
+    while (done < steps) {
+        const long long n = std::min(every, steps - done);
+        if (tmx_step(h, (int)n)) return die("step");
+        done += n;
+        if (tmx_mixing(h, rows.data(), im)) return die("mixing");
+        const double s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        std::printf("step %lld  outlet I_A %.9g I_B %.9g I_C %.9g  %.1f MLUPS\n", done, im[0], im[1], im[2],
+                    nodes * (double)done / s / 1e6);
+        std::fflush(stdout);
+    }
+    if (!out.empty()) {
+        std::string fp = out + "/fields.bin";
+        FILE* f = std::fopen(fp.c_str(), "wb");
+        if (!f) {
+            std::perror(fp.c_str());
+            return 1;
+        }
+        int hdr[8] = {c.inx, c.iny, c.nz, c.mnx, c.mny, c.ia, c.ia + c.mnx - 1, (int)steps};
+        std::fwrite(hdr, sizeof(int), 8, f);
+        for (int box = 0; box < 2; box++) {
+            const size_t n = box == 0 ? (size_t)c.inx * c.iny * c.nz : (size_t)c.mnx * c.mny * c.nz;
+            std::vector<double> buf(n);
+            for (int fld = 0; fld < 7; fld++) {
+                if (tmx_fields(h, box, fld, buf.data())) return die("fields");
+                std::fwrite(buf.data(), sizeof(double), n, f);
+            }
+        }
+        std::fclose(f);
+        std::string mp = out + "/mixing.txt";
+        FILE* m = std::fopen(mp.c_str(), "w");
+        if (!m) {
+            std::perror(mp.c_str());
+            return 1;
+        }
+        for (int r = 0; r < c.mny + c.iny; r++) {
+            const double* o = &rows[(size_t)r * 7];
+            std::fprintf(m, "%d\t%.17g\t%.17g\t%.17g\t%.17g\t%.17g\t%.17g\n", (int)o[0], o[1], o[2], o[3], o[4], o[5],
+                         o[6]);
+        }
+        std::fclose(m);
+    }
+    tmx_destroy(h);
+    return 0;
+}
