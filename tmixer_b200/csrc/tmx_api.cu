@@ -70,8 +70,9 @@ struct tmx_handle {
     int bulk_blocks = 0;
     // the boundary kernel runs on a second stream, concurrently with the bulk
     // kernel (disjoint outputs, read-only shared inputs)
-    cudaStream_t aux = nullptr;
-    cudaEvent_t fork = nullptr, join = nullptr;
+    cudaStream_t aux = nullptr, aux2 = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr, join2 = nullptr;
+    int nface = 0;  // the first nface boundary nodes are face classes
     // one captured step per (state buffer, macroscopic output) combination
     cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
 };
@@ -244,9 +245,11 @@ void free_all(tmx_handle* h)
             }
     if (h->fork) cudaEventDestroy(h->fork);
     if (h->join) cudaEventDestroy(h->join);
-    h->fork = h->join = nullptr;
+    if (h->join2) cudaEventDestroy(h->join2);
+    h->fork = h->join = h->join2 = nullptr;
     if (h->aux) cudaStreamDestroy(h->aux);
-    h->aux = nullptr;
+    if (h->aux2) cudaStreamDestroy(h->aux2);
+    h->aux = h->aux2 = nullptr;
     cudaFree(h->mac);
     cudaFree(h->bnode);
     cudaFree(h->bcls);
@@ -273,17 +276,29 @@ int enqueue_step(tmx_handle* h, int cur, int write_macro, cudaEvent_t* ev)
     double* rcur = h->rho[1 - cur];
     TMX_CK(cudaEventRecord(h->fork, h->stream));
     TMX_CK(cudaStreamWaitEvent(h->aux, h->fork, 0));
+    TMX_CK(cudaStreamWaitEvent(h->aux2, h->fork, 0));
     if (ev) TMX_CK(cudaEventRecord(ev[2], h->aux));
-    if (h->nb > 0)
-        tmx::k_boundary<<<(h->nb + 127) / 128, 128, 0, h->aux>>>(pin, pout, rprev, rcur, h->mac, h->bnode, h->bcls,
-                                                                h->nb, h->uin_d[0], h->uin_d[1], G, h->P,
-                                                                write_macro);
-    if (ev) TMX_CK(cudaEventRecord(ev[3], h->aux));
+    const int nf = h->nface, ne = h->nb - h->nface;
+    const int bt = tmx::kBoundaryThreadsHost;
+    if (nf > 0)
+        tmx::k_boundary_faces<<<(nf + bt - 1) / bt, bt, 0, h->aux>>>(pin, pout, rprev, rcur, h->mac, h->bnode,
+                                                                   h->bcls, nf, h->uin_d[0], h->uin_d[1], G, h->P,
+                                                                   write_macro);
+    if (ne > 0)
+        tmx::k_boundary_edges<<<(ne + bt - 1) / bt, bt, 0, h->aux2>>>(pin, pout, rprev, rcur, h->mac,
+                                                                     h->bnode + nf, h->bcls + nf, ne, h->uin_d[0],
+                                                                     h->uin_d[1], G, h->P, write_macro);
+    TMX_CK(cudaEventRecord(h->join2, h->aux2));
+    if (ev) {  // the boundary time spans both boundary kernels
+        TMX_CK(cudaStreamWaitEvent(h->aux, h->join2, 0));
+        TMX_CK(cudaEventRecord(ev[3], h->aux));
+    }
     TMX_CK(cudaEventRecord(h->join, h->aux));
     if (ev) TMX_CK(cudaEventRecord(ev[0], h->stream));
     tmx::k_bulk<<<h->bulk_blocks, 256, 0, h->stream>>>(pin, pout, rcur, h->mac, G, h->P, write_macro);
     if (ev) TMX_CK(cudaEventRecord(ev[1], h->stream));
     TMX_CK(cudaStreamWaitEvent(h->stream, h->join, 0));
+    TMX_CK(cudaStreamWaitEvent(h->stream, h->join2, 0));
     TMX_CK(cudaGetLastError());
     return TMX_OK;
 }
@@ -453,7 +468,8 @@ int tmx_create(const tmx_case* c, int device, tmx_handle** out)
                         delete h;
                         return fail(TMX_E_INVALID, "internal: boundary node (%d,%d,%d,%d) has no class", b, i, j, k);
                     }
-                    bl.emplace_back(cls, tmx::node_index(G, b, i, j, k));
+                    // faces first, then edges and corners; by class, then node
+                    bl.emplace_back((tmx::is_face_class(cls) ? 0 : 256) + cls, tmx::node_index(G, b, i, j, k));
                     h->class_count[cls]++;
                 }
     std::sort(bl.begin(), bl.end());
@@ -461,8 +477,9 @@ int tmx_create(const tmx_case* c, int device, tmx_handle** out)
     std::vector<int> nodes(bl.size());
     std::vector<unsigned char> cls(bl.size());
     for (size_t t = 0; t < bl.size(); t++) {
-        cls[t] = (unsigned char)bl[t].first;
+        cls[t] = (unsigned char)(bl[t].first & 255);
         nodes[t] = bl[t].second;
+        if (bl[t].first < 256) h->nface++;
     }
 
     auto alloc = [&](void** p, size_t n) -> cudaError_t {
@@ -472,6 +489,8 @@ int tmx_create(const tmx_case* c, int device, tmx_handle** out)
     };
     cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->aux, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->aux2, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->join2, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->join, cudaEventDisableTiming);
     for (int s = 0; s < 2 && e == cudaSuccess; s++) {

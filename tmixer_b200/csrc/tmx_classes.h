@@ -43,4 +43,11 @@ enum BoundaryClass : unsigned char {
     K_NCLASSES
 };
 
+// Inlets, outlet and wall faces (one kernel); edges and corners (the other).
+__host__ __device__ constexpr bool is_face_class(int c)
+{
+    return c == K_INLET1 || c == K_INLET2 || c == K_FACE_YT || c == K_FACE_Y1 || c == K_OUTLET || c == K_FACE_MX1 ||
+           c == K_FACE_MXT || c == K_FACE_ZT || c == K_FACE_Z1;
+}
+
 }  // namespace tmx

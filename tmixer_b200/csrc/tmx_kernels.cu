@@ -239,7 +239,7 @@ __device__ __forceinline__ double sum_but(const double (&v)[19], int a, int d)
 }
 // Zou-He density of the velocity-inlet node (side 0: x=1, side 1: x=inx) as
 // the inlet cases compute it this step (Tmixer.cpp:2612-2615, :2675-2678)
-__device__ double inlet_rho_now(const BCtx& c, int side, int j, int k)
+__device__ __forceinline__ double inlet_rho_now(const BCtx& c, int side, int j, int k)
 {
     double v[19];
     const int x = side == 0 ? 1 : c.G->inx;
@@ -280,7 +280,7 @@ __constant__ CornerSpec kCorner[16] = {
 };
 
 // Corner closure on a local copy (runtime indices; 16 nodes per mixer).
-__device__ __noinline__ void corner_closure(const BCtx& c, int fld, int n, double R, double* t)
+__device__ __forceinline__ void corner_closure(const BCtx& c, int fld, int n, double R, double* t)
 {
     const CornerSpec& s = kCorner[n];
     for (int m = 0; m < 6; m++) t[s.bb[m][0]] = t[s.bb[m][1]];
@@ -305,32 +305,13 @@ __device__ __noinline__ void corner_closure(const BCtx& c, int fld, int n, doubl
 
 // Apply the closure of class `cls` to field fld of the node in c, on v (the
 // node's pulled populations).  Closures follow the reference case by case;
-// the comments give the reference lines.
-__device__ __forceinline__ void closure(const BCtx& c, int cls, int fld, double (&v)[19])
+// the comments give the reference lines.  Face classes (inlets, outlet, walls)
+// and edge/corner classes are separate functions so that each boundary kernel
+// holds only the code of its own classes.
+__device__ __forceinline__ void closure_face(const BCtx& c, int cls, int fld, double (&v)[19])
 {
-    const Geom& G = *c.G;
     const bool flow = fld == 0;
     switch (cls) {
-    case K_EDGE_Y1_ZTOP: {  // Cases 2, 3 (:2030-2342)
-        v[2] = v[4]; v[6] = v[5]; v[7] = v[9]; v[8] = v[10]; v[13] = v[11]; v[14] = v[12]; v[18] = v[16];
-        v[15] = (1.0 / 2.0) * (own_fn(c, fld, 15) + own_fn(c, fld, 17));
-        v[17] = v[15];
-        const double A = (1.0 / 4.0) * (v[1] - v[3]);
-        v[7] = v[9] - A; v[8] = v[10] + A; v[13] = v[11] + A; v[14] = v[12] - A;
-    } break;
-    case K_EDGE_X1_ZTOP: {  // Case 4 (:2343-2476); field C keeps p13 = pn13 (:2474)
-        const double B = 1.0 / 4.0 * (v[2] - v[4]);
-        v[1] = v[3]; v[6] = v[5]; v[7] = v[9] - B; v[10] = v[8] + B; v[14] = v[12]; v[17] = v[15] + B; v[18] = v[16] - B;
-        v[13] = own_fn(c, fld, 13);
-        v[11] = (1.0 / 2.0) * (rprev(c, fld, 0, 1, c.j, G.nz - 1) - sum_but(v, 11, 13));
-        if (fld != 3) v[13] = v[11];
-    } break;
-    case K_EDGE_XT_ZTOP: {  // Case 6 (:2477-2605)
-        const double B = (1.0 / 4.0) * (v[2] - v[4]);
-        v[3] = v[1]; v[6] = v[5]; v[9] = v[7] + B; v[8] = v[10] - B; v[13] = v[11]; v[17] = v[15] + B; v[18] = v[16] - B;
-        v[12] = (1.0 / 2.0) * (rprev(c, fld, 0, G.inx, c.j, G.nz - 1) - sum_but(v, 12, 14));
-        v[14] = v[12];
-    } break;
     case K_INLET1: {  // Inlet1 (:2606-2666)
         if (flow) {
             const double U = uin(c, 0, c.j, c.k);
@@ -428,6 +409,35 @@ __device__ __forceinline__ void closure(const BCtx& c, int cls, int fld, double 
             const double A = (1.0 / 2.0) * (v[1] - v[3] + v[7] - v[8] - v[9] + v[10]);
             v[11] = v[13] - A; v[12] = v[14] + A;
         } else pull_node(c, fld, c.b, c.i, c.j, c.k + 1, v);
+    } break;
+    default: break;
+    }
+}
+
+__device__ __forceinline__ void closure_edge(const BCtx& c, int cls, int fld, double (&v)[19])
+{
+    const Geom& G = *c.G;
+    const bool flow = fld == 0;
+    switch (cls) {
+    case K_EDGE_Y1_ZTOP: {  // Cases 2, 3 (:2030-2342)
+        v[2] = v[4]; v[6] = v[5]; v[7] = v[9]; v[8] = v[10]; v[13] = v[11]; v[14] = v[12]; v[18] = v[16];
+        v[15] = (1.0 / 2.0) * (own_fn(c, fld, 15) + own_fn(c, fld, 17));
+        v[17] = v[15];
+        const double A = (1.0 / 4.0) * (v[1] - v[3]);
+        v[7] = v[9] - A; v[8] = v[10] + A; v[13] = v[11] + A; v[14] = v[12] - A;
+    } break;
+    case K_EDGE_X1_ZTOP: {  // Case 4 (:2343-2476); field C keeps p13 = pn13 (:2474)
+        const double B = 1.0 / 4.0 * (v[2] - v[4]);
+        v[1] = v[3]; v[6] = v[5]; v[7] = v[9] - B; v[10] = v[8] + B; v[14] = v[12]; v[17] = v[15] + B; v[18] = v[16] - B;
+        v[13] = own_fn(c, fld, 13);
+        v[11] = (1.0 / 2.0) * (rprev(c, fld, 0, 1, c.j, G.nz - 1) - sum_but(v, 11, 13));
+        if (fld != 3) v[13] = v[11];
+    } break;
+    case K_EDGE_XT_ZTOP: {  // Case 6 (:2477-2605)
+        const double B = (1.0 / 4.0) * (v[2] - v[4]);
+        v[3] = v[1]; v[6] = v[5]; v[9] = v[7] + B; v[8] = v[10] - B; v[13] = v[11]; v[17] = v[15] + B; v[18] = v[16] - B;
+        v[12] = (1.0 / 2.0) * (rprev(c, fld, 0, G.inx, c.j, G.nz - 1) - sum_but(v, 12, 14));
+        v[14] = v[12];
     } break;
     case K_EDGE_YT_ZT: {  // Case 20 (:4238-4385)
         v[4] = v[2]; v[6] = v[5]; v[17] = v[15];
@@ -589,9 +599,10 @@ __device__ __forceinline__ void closure(const BCtx& c, int cls, int fld, double 
 // The post-closure populations of field fld of the boundary node in c.  A
 // species on a wall face is a zero-gradient copy of an interior node's pulled
 // populations (Tmixer.cpp:2766-4237), so it pulls that node directly.
+template <bool FACES>
 __device__ __forceinline__ void closed_pull(const BCtx& c, int cls, int fld, double (&v)[19])
 {
-    if (fld > 0) {
+    if (FACES && fld > 0) {
         int di = 0, dj = 0, dk = 0;
         switch (cls) {
         case K_FACE_YT: dj = -1; break;
@@ -609,19 +620,29 @@ __device__ __forceinline__ void closed_pull(const BCtx& c, int cls, int fld, dou
         }
     }
     pull_node(c, fld, c.b, c.i, c.j, c.k, v);
-    closure(c, cls, fld, v);
+    if (FACES)
+        closure_face(c, cls, fld, v);
+    else
+        closure_edge(c, cls, fld, v);
 }
 
 // ---------------------------------------------------------------------------
-// boundary nodes
+// boundary nodes: one thread per node of a compact, class-sorted list; FACES
+// selects the list of inlet/outlet/wall-face nodes or of edge/corner nodes.
+// The closed species A and B populations wait in shared memory while the
+// reaction term (which needs both densities) is formed.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_boundary(const double* __restrict__ Pin, double* __restrict__ Pout,
-                                                  const double* __restrict__ Rprev, double* __restrict__ Rcur,
-                                                  double* __restrict__ Mac, const int* __restrict__ bnode,
-                                                  const unsigned char* __restrict__ bcls, int nb,
-                                                  const double* __restrict__ uin1, const double* __restrict__ uin2,
-                                                  Geom G, Phys P, int write_macro)
+constexpr int kBoundaryThreads = 128;
+
+template <bool FACES>
+__device__ __forceinline__ void boundary_body(const double* __restrict__ Pin, double* __restrict__ Pout,
+                                              const double* __restrict__ Rprev, double* __restrict__ Rcur,
+                                              double* __restrict__ Mac, const int* __restrict__ bnode,
+                                              const unsigned char* __restrict__ bcls, int nb,
+                                              const double* __restrict__ uin1, const double* __restrict__ uin2,
+                                              const Geom& G, const Phys& P, int write_macro)
 {
+    __shared__ double stash[2][19][kBoundaryThreads];
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nb) return;
     BCtx c;
@@ -637,12 +658,13 @@ __global__ void __launch_bounds__(128) k_boundary(const double* __restrict__ Pin
     const int cls = bcls[t];
     const long long ps = G.ps;
     const bool outlet = c.b == 1 && c.j == 1;
+    const int tx = threadIdx.x;
 
     double poly[19];
     double rho, ux, uy, uz;
     {
         double f[19];
-        closed_pull(c, cls, 0, f);
+        closed_pull<FACES>(c, cls, 0, f);
         // the outlet row's density is pinned to rho_out (Tmixer.cpp:9575-9582)
         rho = outlet ? P.rho_out : sum19(f);
         double sxm, sym, szm;
@@ -653,25 +675,30 @@ __global__ void __launch_bounds__(128) k_boundary(const double* __restrict__ Pin
         eq_poly(ux, uy, uz, poly);
         collide_store(Pout, ps, c.g, 0, f, rho, poly, P, 0.0);
     }
-    // species densities first (the reaction couples A and B), then each
-    // species' closure again and its collision
-    double ca = 0.0, cb = 0.0, cc = 0.0;
-#pragma unroll 1
-    for (int fld = 1; fld <= 2; fld++) {
+    double ca, cb, cc;
+    {
         double v[19];
-        closed_pull(c, cls, fld, v);
-        const double s = sum19(v);
-        ca = fld == 1 ? s : ca;
-        cb = fld == 2 ? s : cb;
+        closed_pull<FACES>(c, cls, 1, v);
+        ca = sum19(v);
+#pragma unroll
+        for (int q = 0; q < 19; q++) stash[0][q][tx] = v[q];
+        closed_pull<FACES>(c, cls, 2, v);
+        cb = sum19(v);
+#pragma unroll
+        for (int q = 0; q < 19; q++) stash[1][q][tx] = v[q];
     }
     const double rt = P.rateconst * ca * cb;
-#pragma unroll 1
-    for (int fld = 1; fld <= 3; fld++) {
+    {
         double v[19];
-        closed_pull(c, cls, fld, v);
-        if (fld == 3) cc = sum19(v);
-        const double cf = fld == 1 ? ca : (fld == 2 ? cb : cc);
-        collide_store(Pout, ps, c.g, fld, v, cf, poly, P, rt);
+#pragma unroll
+        for (int q = 0; q < 19; q++) v[q] = stash[0][q][tx];
+        collide_store(Pout, ps, c.g, 1, v, ca, poly, P, rt);
+#pragma unroll
+        for (int q = 0; q < 19; q++) v[q] = stash[1][q][tx];
+        collide_store(Pout, ps, c.g, 2, v, cb, poly, P, rt);
+        closed_pull<FACES>(c, cls, 3, v);
+        cc = sum19(v);
+        collide_store(Pout, ps, c.g, 3, v, cc, poly, P, rt);
     }
 
     Rcur[c.g] = rho;
@@ -687,6 +714,24 @@ __global__ void __launch_bounds__(128) k_boundary(const double* __restrict__ Pin
         Mac[5 * ps + c.g] = cb;
         Mac[6 * ps + c.g] = cc;
     }
+}
+
+__global__ void __launch_bounds__(kBoundaryThreads)
+    k_boundary_faces(const double* __restrict__ Pin, double* __restrict__ Pout, const double* __restrict__ Rprev,
+                     double* __restrict__ Rcur, double* __restrict__ Mac, const int* __restrict__ bnode,
+                     const unsigned char* __restrict__ bcls, int nb, const double* __restrict__ uin1,
+                     const double* __restrict__ uin2, Geom G, Phys P, int write_macro)
+{
+    boundary_body<true>(Pin, Pout, Rprev, Rcur, Mac, bnode, bcls, nb, uin1, uin2, G, P, write_macro);
+}
+
+__global__ void __launch_bounds__(kBoundaryThreads)
+    k_boundary_edges(const double* __restrict__ Pin, double* __restrict__ Pout, const double* __restrict__ Rprev,
+                     double* __restrict__ Rcur, double* __restrict__ Mac, const int* __restrict__ bnode,
+                     const unsigned char* __restrict__ bcls, int nb, const double* __restrict__ uin1,
+                     const double* __restrict__ uin2, Geom G, Phys P, int write_macro)
+{
+    boundary_body<false>(Pin, Pout, Rprev, Rcur, Mac, bnode, bcls, nb, uin1, uin2, G, P, write_macro);
 }
 
 // ---------------------------------------------------------------------------
