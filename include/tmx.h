@@ -36,6 +36,8 @@ extern "C" {
 
 /* arithmetic of the state and of the step */
 #define TMX_FP64 0 /* plain form: FP64 storage and arithmetic, bit-exact with the reference */
+#define TMX_FP32 1 /* FP32 storage and arithmetic */
+#define TMX_FP16 2 /* FP32 arithmetic, populations stored in FP16 as f_q - w_q*rho0 (flow) and g_q (species) */
 
 /* field ids of tmx_fields */
 #define TMX_RHO 0
@@ -57,7 +59,8 @@ extern "C" {
  *   c_in[s][n]          Tmixer.cpp:90-97     species s (A,B,C) at inlet n (1,2)
  *   rateconst           Tmixer.cpp:99        A + B -> C rate constant
  *   umean               Tmixer.cpp:107       mean of the inlet-1 duct profile
- *   precision           TMX_FP64
+ *   precision           TMX_FP64, TMX_FP32 or TMX_FP16 (no counterpart in the reference,
+ *                       which is FP64 throughout)
  * Requirements: all sizes >= 3, 2 <= ia, ia + mnx - 1 <= inx - 1. */
 typedef struct tmx_case {
     int inx, iny, nz;

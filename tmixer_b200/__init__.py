@@ -28,7 +28,10 @@ _PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_PKG, "libtmx.so")
 
 FIELDS = ("rho", "ux", "uy", "uz", "cA", "cB", "cC")
-TMX_FP64 = 0
+TMX_FP64 = 0  # plain form, bit-exact with the reference
+TMX_FP32 = 1  # FP32 storage and arithmetic
+TMX_FP16 = 2  # FP32 arithmetic, populations stored in FP16 (flow shifted by w_q*rho0)
+PRECISIONS = {"fp64": TMX_FP64, "fp32": TMX_FP32, "fp16": TMX_FP16}
 ABI_VERSION = 1
 
 _ERRORS = {-1: "invalid", -2: "out of memory", -3: "CUDA error", -4: "bad call order", -5: "non-finite state"}
@@ -171,7 +174,7 @@ def reference_case() -> CaseSpec:
 
 
 def w_layout(W: int, u_max: float, tau_f: float, tau_c: float, k: float, rho: float = 1.0,
-             steps: int = 0) -> CaseSpec:
+             steps: int = 0, precision: int = TMX_FP64) -> CaseSpec:
     """A T-mixer of width W in the layout of the benchmark configurations:
     inlet 8W x W x W, mixing 2W x 4W x W, opening x = 3W+1 .. 5W, species A
     at inlet 1 and B at inlet 2 with c = 1, rho0 = rho_out = rho.  The duct
@@ -180,7 +183,9 @@ def w_layout(W: int, u_max: float, tau_f: float, tau_c: float, k: float, rho: fl
     c = _CCase()
     _check(lib().tmx_case_wlayout(int(W), float(u_max), float(tau_f), float(tau_c), float(k), float(rho),
                                   ctypes.byref(c)))
-    return CaseSpec.from_c(c, steps=steps)
+    spec = CaseSpec.from_c(c, steps=steps)
+    spec.precision = int(precision)
+    return spec
 
 
 class Solver:
@@ -280,4 +285,5 @@ class Solver:
         return dict(nodes=o[0], interior=o[1], boundary=o[2], device_bytes=o[3])
 
 
-__all__ = ["CaseSpec", "Solver", "TmxError", "FIELDS", "reference_case", "w_layout", "lib"]
+__all__ = ["CaseSpec", "Solver", "TmxError", "FIELDS", "TMX_FP64", "TMX_FP32", "TMX_FP16", "PRECISIONS",
+           "reference_case", "w_layout", "lib"]

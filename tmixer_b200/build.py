@@ -17,8 +17,11 @@ CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libtmx.so")
 RUN = os.path.join(PKG, "tmx_run")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC"]
-SOURCES = ["tmx_kernels.cu", "tmx_api.cu"]
+NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC"]
+# per-source contraction: the FP64 kernels and the host code keep every
+# operation separately rounded; the reduced-precision kernels may fuse
+SOURCES = {"tmx_kernels.cu": ["--fmad=false"], "tmx_api.cu": ["--fmad=false"], "tmx_kernels_lp.cu": ["--fmad=true"]}
+OBJDIR = os.path.join(PKG, "_build")
 
 
 def _nvcc() -> str:
@@ -36,14 +39,22 @@ def _stale(target: str, deps: list[str]) -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
-    srcs = [os.path.join(CSRC, s) for s in SOURCES]
-    deps = srcs + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
-    deps.append(os.path.join(ROOT, "include", "tmx.h"))
-    if force or _stale(LIB, deps):
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
+    headers.append(os.path.join(ROOT, "include", "tmx.h"))
+    os.makedirs(OBJDIR, exist_ok=True)
+    objs = []
+    for src, flags in SOURCES.items():
+        path = os.path.join(CSRC, src)
+        obj = os.path.join(OBJDIR, src + ".o")
+        objs.append(obj)
+        if force or _stale(obj, [path] + headers):
+            cmd = [_nvcc()] + NVCC_FLAGS + flags + ARCH + ["-c", "-o", obj, path]
+            if verbose:
+                print(" ".join(cmd), file=sys.stderr)
+            subprocess.run(cmd, check=True)
+    if force or _stale(LIB, objs):
         tmp = LIB + ".tmp"
-        cmd = [_nvcc()] + NVCC_FLAGS + ARCH + ["-shared", "-o", tmp] + srcs
-        if verbose:
-            print(" ".join(cmd), file=sys.stderr)
+        cmd = [_nvcc()] + ARCH + ["-shared", "-o", tmp] + objs
         subprocess.run(cmd, check=True)
         os.replace(tmp, LIB)
     drv = os.path.join(CSRC, "tmx_run.cpp")

@@ -51,13 +51,14 @@ struct tmx_handle {
     Phys P;
     int device = 0;
     cudaStream_t stream = nullptr;
-    double* pop[2] = {nullptr, nullptr};
-    double* rho[2] = {nullptr, nullptr};
+    // populations (storage type of the form) and densities (its arithmetic type)
+    void* pop[2] = {nullptr, nullptr};
+    void* rho[2] = {nullptr, nullptr};
     double* mac = nullptr;
     int* bnode = nullptr;
     unsigned char* bcls = nullptr;
     int nb = 0;
-    double* uin_d[2] = {nullptr, nullptr};
+    void* uin_d[2] = {nullptr, nullptr};
     double* stats = nullptr;
     double* partial = nullptr;
     std::vector<double> uin1, uin2;
@@ -75,11 +76,40 @@ struct tmx_handle {
     int nface = 0;  // the first nface boundary nodes are face classes
     // one captured step per (state buffer, macroscopic output) combination
     cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    int sbytes = 8, tbytes = 8;  // storage / arithmetic bytes per value of the form
+    const struct StepKernels* K = nullptr;
+};
+
+// the step kernels of one form
+struct StepKernels {
+    void (*init)(void*, void*, double*, Geom, Phys, double);
+    void (*bulk)(const void*, void*, void*, double*, Geom, Phys, int);
+    void (*faces)(const void*, void*, const void*, void*, double*, const int*, const unsigned char*, int, const void*,
+                  const void*, Geom, Phys, int);
+    void (*edges)(const void*, void*, const void*, void*, double*, const int*, const unsigned char*, int, const void*,
+                  const void*, Geom, Phys, int);
+    int sbytes, tbytes;
+};
+static const StepKernels kForms[3] = {
+    {tmx::k_init_f64, tmx::k_bulk_f64, tmx::k_bfaces_f64, tmx::k_bedges_f64, 8, 8},
+    {tmx::k_init_f32, tmx::k_bulk_f32, tmx::k_bfaces_f32, tmx::k_bedges_f32, 4, 4},
+    {tmx::k_init_f16, tmx::k_bulk_f16, tmx::k_bfaces_f16, tmx::k_bedges_f16, 2, 4},
 };
 
 namespace {
 
 constexpr int kSumBlocks = 592;
+
+// IEEE binary16 bits to float (host side of tmx_populations)
+float half_bits_to_float(unsigned short h)
+{
+    const unsigned sign = (h >> 15) & 1u, exp = (h >> 10) & 31u, man = h & 1023u;
+    float v;
+    if (exp == 0) v = std::ldexp((float)man, -24);
+    else if (exp == 31) v = man ? NAN : INFINITY;
+    else v = std::ldexp((float)(man | 1024u), (int)exp - 25);
+    return sign ? -v : v;
+}
 
 void geometry_of(const tmx_case& c, Geom& G)
 {
@@ -109,18 +139,22 @@ void physics_of(const tmx_case& c, Phys& P)
     }
     P.rateconst = c.rateconst;
     P.rho_out = c.rho_out;
+    // reduced-precision storage keeps f_q - w_q*rho0 for the flow; species unshifted
+    P.ref[0] = c.rho0;
+    P.ref[1] = P.ref[2] = P.ref[3] = 0.0;
     for (int s = 0; s < 3; s++)
         for (int n = 0; n < 2; n++) P.cin[s][n] = c.c_in[s][n];
 }
 
-long long footprint(const Geom& G, long long nb)
+long long footprint(const Geom& G, long long nb, int precision)
 {
+    const StepKernels& K = kForms[precision];
     long long b = 0;
-    b += 2LL * 76 * G.ps * 8;  // populations
-    b += 2LL * 4 * G.ps * 8;   // densities
+    b += 2LL * 76 * G.ps * K.sbytes;  // populations
+    b += 2LL * 4 * G.ps * K.tbytes;   // densities
     b += 7LL * G.ps * 8;       // macroscopic fields
     b += nb * 5;               // boundary list
-    b += 2LL * (G.iny + 3) * (G.nz + 3) * 8;
+    b += 2LL * (G.iny + 3) * (G.nz + 3) * K.tbytes;
     b += (long long)(G.mny + G.iny) * 9 * 8 + kSumBlocks * 6 * 8;
     return b;
 }
@@ -270,10 +304,10 @@ void free_all(tmx_handle* h)
 int enqueue_step(tmx_handle* h, int cur, int write_macro, cudaEvent_t* ev)
 {
     const Geom& G = h->G;
-    const double* pin = h->pop[cur];
-    double* pout = h->pop[1 - cur];
-    const double* rprev = h->rho[cur];
-    double* rcur = h->rho[1 - cur];
+    const void* pin = h->pop[cur];
+    void* pout = h->pop[1 - cur];
+    const void* rprev = h->rho[cur];
+    void* rcur = h->rho[1 - cur];
     TMX_CK(cudaEventRecord(h->fork, h->stream));
     TMX_CK(cudaStreamWaitEvent(h->aux, h->fork, 0));
     TMX_CK(cudaStreamWaitEvent(h->aux2, h->fork, 0));
@@ -281,11 +315,11 @@ int enqueue_step(tmx_handle* h, int cur, int write_macro, cudaEvent_t* ev)
     const int nf = h->nface, ne = h->nb - h->nface;
     const int bt = tmx::kBoundaryThreadsHost;
     if (nf > 0)
-        tmx::k_boundary_faces<<<(nf + bt - 1) / bt, bt, 0, h->aux>>>(pin, pout, rprev, rcur, h->mac, h->bnode,
+        h->K->faces<<<(nf + bt - 1) / bt, bt, 0, h->aux>>>(pin, pout, rprev, rcur, h->mac, h->bnode,
                                                                    h->bcls, nf, h->uin_d[0], h->uin_d[1], G, h->P,
                                                                    write_macro);
     if (ne > 0)
-        tmx::k_boundary_edges<<<(ne + bt - 1) / bt, bt, 0, h->aux2>>>(pin, pout, rprev, rcur, h->mac,
+        h->K->edges<<<(ne + bt - 1) / bt, bt, 0, h->aux2>>>(pin, pout, rprev, rcur, h->mac,
                                                                      h->bnode + nf, h->bcls + nf, ne, h->uin_d[0],
                                                                      h->uin_d[1], G, h->P, write_macro);
     TMX_CK(cudaEventRecord(h->join2, h->aux2));
@@ -295,7 +329,7 @@ int enqueue_step(tmx_handle* h, int cur, int write_macro, cudaEvent_t* ev)
     }
     TMX_CK(cudaEventRecord(h->join, h->aux));
     if (ev) TMX_CK(cudaEventRecord(ev[0], h->stream));
-    tmx::k_bulk<<<h->bulk_blocks, 256, 0, h->stream>>>(pin, pout, rcur, h->mac, G, h->P, write_macro);
+    h->K->bulk<<<h->bulk_blocks, 256, 0, h->stream>>>(pin, pout, rcur, h->mac, G, h->P, write_macro);
     if (ev) TMX_CK(cudaEventRecord(ev[1], h->stream));
     TMX_CK(cudaStreamWaitEvent(h->stream, h->join, 0));
     TMX_CK(cudaStreamWaitEvent(h->stream, h->join2, 0));
@@ -419,7 +453,8 @@ int tmx_case_check(const tmx_case* c)
     if (!std::isfinite(c->rho0) || !(c->rho0 > 0) || !std::isfinite(c->rho_out) || !(c->rho_out > 0))
         return fail(TMX_E_INVALID, "rho0 and rho_out must be finite and positive");
     if (!std::isfinite(c->umean) || !std::isfinite(c->rateconst)) return fail(TMX_E_INVALID, "non-finite parameter");
-    if (c->precision != TMX_FP64) return fail(TMX_E_INVALID, "unsupported precision %d", c->precision);
+    if (c->precision < TMX_FP64 || c->precision > TMX_FP16)
+        return fail(TMX_E_INVALID, "unsupported precision %d", c->precision);
     const long long n = (long long)c->inx * c->iny * c->nz + (long long)c->mnx * c->mny * c->nz;
     if (n > 2000000000LL / 1) return fail(TMX_E_INVALID, "too many nodes (%lld)", n);
     return TMX_OK;
@@ -432,7 +467,7 @@ int tmx_case_footprint(const tmx_case* c, long long* bytes)
     if (!bytes) return fail(TMX_E_INVALID, "null output");
     Geom G;
     geometry_of(*c, G);
-    *bytes = footprint(G, boundary_count(G));
+    *bytes = footprint(G, boundary_count(G), c->precision);
     return TMX_OK;
 }
 
@@ -452,6 +487,9 @@ int tmx_create(const tmx_case* c, int device, tmx_handle** out)
     h->device = device;
     geometry_of(*c, h->G);
     physics_of(*c, h->P);
+    h->K = &kForms[c->precision];
+    h->sbytes = h->K->sbytes;
+    h->tbytes = h->K->tbytes;
     const Geom& G = h->G;
 
     // boundary node list, sorted by class then node index
@@ -494,9 +532,9 @@ int tmx_create(const tmx_case* c, int device, tmx_handle** out)
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->join, cudaEventDisableTiming);
     for (int s = 0; s < 2 && e == cudaSuccess; s++) {
-        e = alloc((void**)&h->pop[s], (size_t)76 * G.ps * sizeof(double));
-        if (e == cudaSuccess) e = alloc((void**)&h->rho[s], (size_t)4 * G.ps * sizeof(double));
-        if (e == cudaSuccess) e = alloc((void**)&h->uin_d[s], (size_t)(G.iny + 3) * (G.nz + 3) * sizeof(double));
+        e = alloc((void**)&h->pop[s], (size_t)76 * G.ps * h->sbytes);
+        if (e == cudaSuccess) e = alloc((void**)&h->rho[s], (size_t)4 * G.ps * h->tbytes);
+        if (e == cudaSuccess) e = alloc((void**)&h->uin_d[s], (size_t)(G.iny + 3) * (G.nz + 3) * h->tbytes);
     }
     if (e == cudaSuccess) e = alloc((void**)&h->mac, (size_t)7 * G.ps * sizeof(double));
     if (e == cudaSuccess) e = alloc((void**)&h->bnode, std::max<size_t>(1, nodes.size()) * sizeof(int));
@@ -525,12 +563,18 @@ int tmx_init(tmx_handle* h)
     if (!h) return fail(TMX_E_INVALID, "null handle");
     TMX_CK(cudaSetDevice(h->device));
     inlet_profile(h->c, h->uin1, h->uin2);
-    const size_t nu = h->uin1.size() * sizeof(double);
-    TMX_CK(cudaMemcpyAsync(h->uin_d[0], h->uin1.data(), nu, cudaMemcpyHostToDevice, h->stream));
-    TMX_CK(cudaMemcpyAsync(h->uin_d[1], h->uin2.data(), nu, cudaMemcpyHostToDevice, h->stream));
+    if (h->tbytes == 8) {
+        const size_t nu = h->uin1.size() * sizeof(double);
+        TMX_CK(cudaMemcpy(h->uin_d[0], h->uin1.data(), nu, cudaMemcpyHostToDevice));
+        TMX_CK(cudaMemcpy(h->uin_d[1], h->uin2.data(), nu, cudaMemcpyHostToDevice));
+    } else {
+        std::vector<float> a(h->uin1.begin(), h->uin1.end()), b(h->uin2.begin(), h->uin2.end());
+        TMX_CK(cudaMemcpy(h->uin_d[0], a.data(), a.size() * sizeof(float), cudaMemcpyHostToDevice));
+        TMX_CK(cudaMemcpy(h->uin_d[1], b.data(), b.size() * sizeof(float), cudaMemcpyHostToDevice));
+    }
     h->cur = 0;
     h->rcur = 0;
-    tmx::k_init<<<h->bulk_blocks, 256, 0, h->stream>>>(h->pop[0], h->rho[0], h->mac, h->G, h->P, h->c.rho0);
+    h->K->init<<<h->bulk_blocks, 256, 0, h->stream>>>(h->pop[0], h->rho[0], h->mac, h->G, h->P, h->c.rho0);
     TMX_CK(cudaGetLastError());
     TMX_CK(cudaStreamSynchronize(h->stream));
     h->steps = 0;
@@ -598,9 +642,38 @@ int tmx_populations(tmx_handle* h, int box, int fld, double* host_out)
     const Geom& G = h->G;
     const size_t n = (size_t)G.nx[box] * G.ny[box] * G.nz;
     std::vector<double> stage;
+    if (h->sbytes == 8) {
+        for (int q = 0; q < 19; q++) {
+            const double* src = (const double*)h->pop[h->cur] + (size_t)(fld * 19 + q) * G.ps;
+            int rc = box_to_host(h, box, src, host_out + q * n, stage);
+            if (rc) return rc;
+        }
+        return TMX_OK;
+    }
+    // reduced precision: widen (and add back the storage shift) on the host
+    std::vector<double> wide(n);
+    std::vector<unsigned char> raw(n * h->sbytes);
+    const double w[3] = {1.0 / 3.0, 1.0 / 18.0, 1.0 / 36.0};
     for (int q = 0; q < 19; q++) {
-        int rc = box_to_host(h, box, h->pop[h->cur] + (size_t)(fld * 19 + q) * G.ps, host_out + q * n, stage);
-        if (rc) return rc;
+        const unsigned char* src = (const unsigned char*)h->pop[h->cur] + ((size_t)(fld * 19 + q) * G.ps + G.base[box]) * h->sbytes;
+        TMX_CK(cudaMemcpy(raw.data(), src, raw.size(), cudaMemcpyDeviceToHost));
+        const float sh = (float)(q == 0 ? w[0] : (q <= 6 ? w[1] : w[2])) * (float)h->P.ref[fld];
+        for (size_t t = 0; t < n; t++) {
+            float v;
+            if (h->sbytes == 4) {
+                std::memcpy(&v, &raw[t * 4], 4);
+            } else {
+                unsigned short hb;
+                std::memcpy(&hb, &raw[t * 2], 2);
+                v = half_bits_to_float(hb) + sh;
+            }
+            wide[t] = v;
+        }
+        const int nx = G.nx[box], ny = G.ny[box], nz = G.nz;
+        for (int k = 0; k < nz; k++)
+            for (int j = 0; j < ny; j++)
+                for (int i = 0; i < nx; i++)
+                    host_out[q * n + ((size_t)i * ny + j) * nz + k] = wide[((size_t)k * ny + j) * nx + i];
     }
     return TMX_OK;
 }

@@ -46,6 +46,7 @@ struct Phys {
     double rateconst;
     double rho_out;
     double cin[3][2];
+    double ref[4];  // storage shift of the reduced-precision forms: f_q is kept as f_q - w_q*ref[field]
 };
 
 __host__ __device__ inline bool is_boundary(const Geom& G, int b, int i, int j, int k)
@@ -131,34 +132,37 @@ __device__ __forceinline__ double wq(int q) { return q == 0 ? 1.0 / 3.0 : (q <= 
 // by 0 and +-1 are exact and adding a zero changes at most the sign of a zero
 // result (which the equilibrium polynomial absorbs), so only the sum of the
 // two non-zero terms rounds; q is a compile-time constant after unrolling.
-__device__ __forceinline__ double e_dot_u(int q, double ux, double uy, double uz)
+template <class T>
+__device__ __forceinline__ T e_dot_u(int q, T ux, T uy, T uz)
 {
-    const double a = EX(q) > 0 ? ux : -ux, b = EY(q) > 0 ? uy : -uy, c = EZ(q) > 0 ? uz : -uz;
+    const T a = EX(q) > 0 ? ux : -ux, b = EY(q) > 0 ? uy : -uy, c = EZ(q) > 0 ? uz : -uz;
     if (EX(q) != 0) return EY(q) != 0 ? a + b : (EZ(q) != 0 ? a + c : a);
     if (EY(q) != 0) return EZ(q) != 0 ? b + c : b;
-    return EZ(q) != 0 ? c : 0.0;
+    return EZ(q) != 0 ? c : T(0);
 }
 
 // Equilibrium polynomial shared by the four fields (they use the flow
 // velocity; Tmixer.cpp:1602-1830):
 //   q=0:  1.0 - 3.0*u2/2.0
 //   q>0:  1.0 + 3.0*eu - 3.0*u2/2.0 + 9.0*eu*eu/2.0   (C left-to-right)
-__device__ __forceinline__ void eq_poly(double ux, double uy, double uz, double (&poly)[19])
+template <class T>
+__device__ __forceinline__ void eq_poly(T ux, T uy, T uz, T (&poly)[19])
 {
-    const double u2 = ux * ux + uy * uy + uz * uz;
-    const double t = 3.0 * u2 / 2.0;
-    poly[0] = 1.0 - t;
+    const T u2 = ux * ux + uy * uy + uz * uz;
+    const T t = T(3) * u2 / T(2);
+    poly[0] = T(1) - t;
 #pragma unroll
     for (int q = 1; q < 19; q++) {
-        const double eu = e_dot_u(q, ux, uy, uz);
-        poly[q] = 1.0 + 3.0 * eu - t + 9.0 * eu * eu / 2.0;
+        const T eu = e_dot_u(q, ux, uy, uz);
+        poly[q] = T(1) + T(3) * eu - t + T(9) * eu * eu / T(2);
     }
 }
 
 // rho = f0 + f1 + ... + f18 in index order (Tmixer.cpp:9391-9560)
-__device__ __forceinline__ double sum19(const double (&v)[19])
+template <class T>
+__device__ __forceinline__ T sum19(const T (&v)[19])
 {
-    double s = v[0];
+    T s = v[0];
 #pragma unroll
     for (int q = 1; q < 19; q++) s += v[q];
     return s;
@@ -166,7 +170,8 @@ __device__ __forceinline__ double sum19(const double (&v)[19])
 
 // momentum sums in index order; zero components drop out exactly
 // (Tmixer.cpp:9597-9609)
-__device__ __forceinline__ void momentum(const double (&f)[19], double& sx, double& sy, double& sz)
+template <class T>
+__device__ __forceinline__ void momentum(const T (&f)[19], T& sx, T& sy, T& sz)
 {
     sx = f[1] - f[3] + f[7] - f[8] - f[9] + f[10] + f[11] - f[12] - f[13] + f[14];
     sy = f[2] - f[4] + f[7] + f[8] - f[9] - f[10] + f[15] - f[16] - f[17] + f[18];

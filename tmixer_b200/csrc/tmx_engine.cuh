@@ -1,0 +1,816 @@
+// tmx_engine.cuh -- the T-mixer step as device code templated on a precision
+// policy PR (scalar type T of the arithmetic, storage type S of the
+// populations).  The kernels that instantiate it live in tmx_kernels.cu (FP64,
+// compiled without contraction: bit-exact with the reference) and
+// tmx_kernels_lp.cu (FP32 arithmetic, FP32 or shifted-FP16 storage).
+//
+// One step of the reference (equilibrium, collision, streaming,
+// boundary_conditions, calculate_velocity_density; Tmixer.cpp:10469-10475)
+// runs as launches over disjoint node sets:
+//
+//   bulk      every node that no boundary case touches: pull the 76
+//             post-collision populations of the previous step from their
+//             upstream neighbours, take moments, equilibrium, BGK collision
+//             plus reaction, write the 76 new post-collision populations.
+//   boundary  every boundary node (compact list, sorted by case; faces and
+//             edges/corners in two kernels): the same, with the reference's
+//             closure for its case between the pull and the moments.
+//
+// The state between steps is the post-collision population set (the
+// reference's fn/gn/hn/pn), double-buffered (A-B pull).  Boundary closures
+// read, besides their own pulled populations: their own post-collision
+// values ("undo streaming"), the previous step's densities of a few nodes
+// (kept in R, written by both kernels for the nodes that are read), the
+// current step's flow density of an inlet node (recomputed from that node's
+// pulled populations), and the pulled species populations of an interior
+// node (zero-gradient copies).  None of these is written during the step, so
+// all boundary nodes run in parallel and the kernels need no ordering.
+#pragma once
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include "tmx_classes.h"
+#include "tmx_device.cuh"
+
+namespace tmx {
+
+// ---------------------------------------------------------------------------
+// precision policies
+// ---------------------------------------------------------------------------
+
+// Plain form: FP64 storage and arithmetic, operation by operation as the
+// reference (the translation unit is compiled with --fmad=false); the
+// equilibrium divisions are correctly rounded (div_c).
+struct F64 {
+    using T = double;
+    using S = double;
+    __device__ static T load(const S* p, T) { return __ldg(p); }
+    __device__ static void store(S* p, T v, T) { *p = v; }
+    __device__ static T shift(int, int, const Phys&) { return 0.0; }
+    __device__ static bool tiny(T r) { return tiny_density(r); }
+    __device__ static T feq(T x, int q, bool tiny) { return tiny ? feq_div_exact(x, q) : feq_div(x, q); }
+};
+
+// FP32 arithmetic and storage (no shift).
+struct F32 {
+    using T = float;
+    using S = float;
+    __device__ static T load(const S* p, T) { return __ldg(p); }
+    __device__ static void store(S* p, T v, T) { *p = v; }
+    __device__ static T shift(int, int, const Phys&) { return 0.0f; }
+    __device__ static bool tiny(T) { return false; }
+    __device__ static T feq(T x, int q, bool) { return x * (float)wq(q); }
+};
+
+// FP32 arithmetic on populations stored in FP16 as f_q - w_q*ref[field]
+// (ref = rho0 for the flow, so only the deviation from rest is stored).
+struct F16 {
+    using T = float;
+    using S = __half;
+    __device__ static T load(const S* p, T sh) { return __half2float(__ldg(p)) + sh; }
+    __device__ static void store(S* p, T v, T sh) { *p = __float2half_rn(v - sh); }
+    __device__ static T shift(int fld, int q, const Phys& P) { return (float)wq(q) * (float)P.ref[fld]; }
+    __device__ static bool tiny(T) { return false; }
+    __device__ static T feq(T x, int q, bool) { return x * (float)wq(q); }
+};
+
+// ---------------------------------------------------------------------------
+// per-node physics: equilibrium -> collision -> store
+// ---------------------------------------------------------------------------
+
+// Collide one field given its populations f, density r and the shared
+// equilibrium polynomial, and store the result.  The reaction source of
+// Tmixer.cpp:9697-9761: species A and B (fld 1, 2) lose (w_q*rt)*1.0, C gains
+// (w_q*rt)*2.0 (molecular weights Ma = Mb = 1, Mp = 2, :9667).  fld may be a
+// run-time value; the arithmetic is the same either way.
+template <class PR>
+__device__ __forceinline__ void collide_store(typename PR::S* __restrict__ Pout, long long ps, int g, int fld,
+                                              const typename PR::T (&f)[19], typename PR::T r,
+                                              const typename PR::T (&poly)[19], const Phys& P, typename PR::T rt)
+{
+    using T = typename PR::T;
+    const T c1 = T(P.c1[fld]), c2 = T(P.c2[fld]);
+    typename PR::S* out = Pout + (long long)fld * 19 * ps + g;
+    const bool tiny = PR::tiny(r);
+#pragma unroll
+    for (int q = 0; q < 19; q++) {
+        const T feq = PR::feq(r * poly[q], q, tiny);
+        T v = f[q] * c1 + c2 * feq;
+        if (fld == 1 || fld == 2) v = v - T(wq(q)) * rt;
+        if (fld == 3) v = v + (T(wq(q)) * rt) * T(2);
+        PR::store(out + (long long)q * ps, v, PR::shift(fld, q, P));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// initial state: f = feq(rho0, 0) for the flow and 0 for the species
+// (Tmixer.cpp:1544-1585, 1835-2018), then the first step's collision.
+// ---------------------------------------------------------------------------
+template <class PR>
+__device__ __forceinline__ void init_node(typename PR::S* __restrict__ Pout, typename PR::T* __restrict__ R,
+                                          double* __restrict__ Mac, const Geom& G, const Phys& P, double rho0d, int g)
+{
+    using T = typename PR::T;
+    const long long ps = G.ps;
+    const T rho0 = T(rho0d);
+    T poly[19];
+    eq_poly(T(0), T(0), T(0), poly);
+    T f[19], z[19];
+#pragma unroll
+    for (int q = 0; q < 19; q++) {
+        const T d = q == 0 ? T(3) : (q <= 6 ? T(18) : T(36));
+        f[q] = (rho0 * poly[q]) / d;
+        z[q] = (T(0) * poly[q]) / d;
+    }
+    const T rt = T(P.rateconst) * T(0) * T(0);
+    collide_store<PR>(Pout, ps, g, 0, f, rho0, poly, P, rt);
+    collide_store<PR>(Pout, ps, g, 1, z, T(0), poly, P, rt);
+    collide_store<PR>(Pout, ps, g, 2, z, T(0), poly, P, rt);
+    collide_store<PR>(Pout, ps, g, 3, z, T(0), poly, P, rt);
+    R[g] = rho0;
+    R[ps + g] = T(0);
+    R[2 * ps + g] = T(0);
+    R[3 * ps + g] = T(0);
+    Mac[g] = rho0d;
+#pragma unroll
+    for (int m = 1; m < 7; m++) Mac[m * ps + g] = 0.0;
+}
+
+// ---------------------------------------------------------------------------
+// interior nodes
+// ---------------------------------------------------------------------------
+
+// Upstream node of direction q for an interior node: the lattice neighbour in
+// the same box, or across the opening for the inlet's row 1 (iface 1: ey = +1
+// from mixing row mny) and the mixing box's row mny (iface 2: ey = -1 from
+// inlet row 1).  q is a compile-time constant after unrolling.
+__device__ __forceinline__ int bulk_src(const Geom& G, int g, int i, int k, int sy, int sz, int iface, int q)
+{
+    if (EY(q) == 1 && iface == 1) return G.base[1] + ((k - 1 - EZ(q)) * G.mny + (G.mny - 1)) * G.mnx + (i - G.ia - EX(q));
+    if (EY(q) == -1 && iface == 2) return ((k - 1 - EZ(q)) * G.iny) * G.inx + (i + G.ia - 2 - EX(q));
+    return g - (EX(q) + EY(q) * sy + EZ(q) * sz);
+}
+
+template <class PR>
+__device__ __forceinline__ void bulk_load(const typename PR::S* __restrict__ Pin, long long ps, int fld,
+                                          const Geom& G, const Phys& P, int g, int i, int k, int sy, int sz,
+                                          int iface, typename PR::T (&v)[19])
+{
+    const typename PR::S* base = Pin + (long long)fld * 19 * ps;
+#pragma unroll
+    for (int q = 0; q < 19; q++)
+        v[q] = PR::load(base + (long long)q * ps + bulk_src(G, g, i, k, sy, sz, iface, q), PR::shift(fld, q, P));
+}
+
+// One interior node; returns false for a boundary node (left to the boundary
+// kernels).
+template <class PR>
+__device__ __forceinline__ void bulk_node(const typename PR::S* __restrict__ Pin, typename PR::S* __restrict__ Pout,
+                                          typename PR::T* __restrict__ Rcur, double* __restrict__ Mac, const Geom& G,
+                                          const Phys& P, int write_macro, int g)
+{
+    using T = typename PR::T;
+    const long long ps = G.ps;
+    int b, i, j, k;
+    decode(G, g, b, i, j, k);
+    if (is_boundary(G, b, i, j, k)) return;
+    const int sy = G.nx[b], sz = G.nx[b] * G.ny[b];
+    const int iface = (b == 0 && j == 1) ? 1 : ((b == 1 && j == G.mny) ? 2 : 0);
+
+    // flow: moments, equilibrium polynomial (shared by all four fields: they
+    // use the flow velocity, Tmixer.cpp:1602-1830), collision
+    T poly[19];
+    T rho, ux, uy, uz;
+    {
+        T f[19];
+        bulk_load<PR>(Pin, ps, 0, G, P, g, i, k, sy, sz, iface, f);
+        rho = sum19(f);
+        T sxm, sym, szm;
+        momentum(f, sxm, sym, szm);
+        ux = sxm / rho;
+        uy = sym / rho;
+        uz = szm / rho;
+        eq_poly(ux, uy, uz, poly);
+        collide_store<PR>(Pout, ps, g, 0, f, rho, poly, P, T(0));
+    }
+    // species A and B: the reaction needs both densities before either
+    // collides, so their populations are loaded twice (the second time from
+    // cache) rather than held in registers
+    T ca, cb;
+    {
+        T a[19];
+        bulk_load<PR>(Pin, ps, 1, G, P, g, i, k, sy, sz, iface, a);
+        ca = sum19(a);
+        bulk_load<PR>(Pin, ps, 2, G, P, g, i, k, sy, sz, iface, a);
+        cb = sum19(a);
+    }
+    const T rt = T(P.rateconst) * ca * cb;
+    T cc;
+    {
+        T a[19];
+        bulk_load<PR>(Pin, ps, 1, G, P, g, i, k, sy, sz, iface, a);
+        collide_store<PR>(Pout, ps, g, 1, a, ca, poly, P, rt);
+        bulk_load<PR>(Pin, ps, 2, G, P, g, i, k, sy, sz, iface, a);
+        collide_store<PR>(Pout, ps, g, 2, a, cb, poly, P, rt);
+        bulk_load<PR>(Pin, ps, 3, G, P, g, i, k, sy, sz, iface, a);
+        cc = sum19(a);
+        collide_store<PR>(Pout, ps, g, 3, a, cc, poly, P, rt);
+    }
+    // densities the junction edges read next step (Tmixer.cpp:8609, :8851)
+    if (b == 0 && j == 2 && (i == G.ia || i == G.ib)) {
+        Rcur[g] = rho;
+        Rcur[ps + g] = ca;
+        Rcur[2 * ps + g] = cb;
+        Rcur[3 * ps + g] = cc;
+    }
+    if (write_macro) {
+        Mac[g] = rho;
+        Mac[ps + g] = ux;
+        Mac[2 * ps + g] = uy;
+        Mac[3 * ps + g] = uz;
+        Mac[4 * ps + g] = ca;
+        Mac[5 * ps + g] = cb;
+        Mac[6 * ps + g] = cc;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// boundary closures (Tmixer.cpp:2023-9033)
+// ---------------------------------------------------------------------------
+template <class PR>
+struct BCtx {
+    using T = typename PR::T;
+    const typename PR::S* __restrict__ Pin;
+    const T* __restrict__ Rprev;
+    const T* __restrict__ uin1;
+    const T* __restrict__ uin2;
+    const Geom* G;
+    const Phys* P;
+    long long ps;
+    int g, b, i, j, k;
+};
+
+template <class PR>
+__device__ __forceinline__ typename PR::T own_fn(const BCtx<PR>& c, int fld, int q)
+{
+    return PR::load(c.Pin + (long long)(fld * 19 + q) * c.ps + c.g, PR::shift(fld, q, *c.P));
+}
+template <class PR>
+__device__ __forceinline__ typename PR::T rprev(const BCtx<PR>& c, int fld, int b, int i, int j, int k)
+{
+    return __ldg(c.Rprev + (long long)fld * c.ps + node_index(*c.G, b, i, j, k));
+}
+template <class PR>
+__device__ __forceinline__ typename PR::T uin(const BCtx<PR>& c, int side, int j, int k)
+{
+    return __ldg((side == 0 ? c.uin1 : c.uin2) + j * (c.G->nz + 3) + k);
+}
+template <class PR>
+__device__ __forceinline__ void pull_node(const BCtx<PR>& c, int fld, int b, int i, int j, int k,
+                                          typename PR::T (&v)[19])
+{
+    using T = typename PR::T;
+    const typename PR::S* base = c.Pin + (long long)fld * 19 * c.ps;
+#pragma unroll
+    for (int q = 0; q < 19; q++) {
+        const int s = pull_src(*c.G, b, i, j, k, q);
+        v[q] = s >= 0 ? PR::load(base + (long long)q * c.ps + s, PR::shift(fld, q, *c.P)) : T(0);
+    }
+}
+// the same sum as sum19 without two directions (the closures' "rho - (...)")
+template <class T>
+__device__ __forceinline__ T sum_but(const T (&v)[19], int a, int d)
+{
+    T s = T(0);
+    bool first = true;
+#pragma unroll
+    for (int q = 0; q < 19; q++) {
+        if (q == a || q == d) continue;
+        s = first ? v[q] : s + v[q];
+        first = false;
+    }
+    return s;
+}
+// Zou-He density of the velocity-inlet node (side 0: x=1, side 1: x=inx) as
+// the inlet cases compute it this step (Tmixer.cpp:2612-2615, :2675-2678)
+template <class PR>
+__device__ __forceinline__ typename PR::T inlet_rho_now(const BCtx<PR>& c, int side, int j, int k)
+{
+    using T = typename PR::T;
+    T v[19];
+    const int x = side == 0 ? 1 : c.G->inx;
+    pull_node(c, 0, 0, x, j, k, v);
+    const T U = uin(c, side, j, k);
+    if (side == 0)
+        return (T(1) / (T(1) - U)) * ((v[0] + v[2] + v[4] + v[5] + v[6] + v[15] + v[16] + v[17] + v[18]) +
+                                    T(2) * (v[3] + v[8] + v[9] + v[12] + v[13]));
+    return (T(1) / (T(1) + (U))) * ((v[0] + v[2] + v[4] + v[5] + v[6] + v[15] + v[16] + v[17] + v[18]) +
+                                  T(2) * (v[1] + v[7] + v[10] + v[11] + v[14]));
+}
+
+// corners: six bounce-backs, buried pairs averaged from their own
+// post-collision values, and (corners 1-12) one pair closed from a density.
+struct CornerSpec {
+    signed char bb[6][2];
+    signed char navg;
+    signed char avg[3][2];
+    signed char cp[2];
+};
+static __constant__ CornerSpec kCorner[16] = {
+    {{{1, 3}, {4, 2}, {6, 5}, {10, 8}, {14, 12}, {17, 15}}, 2, {{9, 7}, {11, 13}, {0, 0}}, {16, 18}},    // 1 G'
+    {{{3, 1}, {4, 2}, {6, 5}, {17, 15}, {13, 11}, {9, 7}}, 2, {{10, 8}, {12, 14}, {0, 0}}, {16, 18}},    // 2 F'
+    {{{1, 3}, {2, 4}, {6, 5}, {7, 9}, {18, 16}, {14, 12}}, 2, {{10, 8}, {11, 13}, {0, 0}}, {15, 17}},    // 3 H'
+    {{{3, 1}, {2, 4}, {6, 5}, {8, 10}, {13, 11}, {18, 16}}, 2, {{9, 7}, {12, 14}, {0, 0}}, {15, 17}},    // 4 E'
+    {{{1, 3}, {4, 2}, {5, 6}, {16, 18}, {11, 13}, {10, 8}}, 2, {{9, 7}, {14, 12}, {0, 0}}, {15, 17}},    // 5 G
+    {{{3, 1}, {4, 2}, {5, 6}, {9, 7}, {12, 14}, {16, 18}}, 2, {{10, 8}, {11, 13}, {0, 0}}, {15, 17}},    // 6 F
+    {{{1, 3}, {2, 4}, {5, 6}, {7, 9}, {11, 13}, {15, 17}}, 2, {{10, 8}, {12, 14}, {0, 0}}, {16, 18}},    // 7 H
+    {{{3, 1}, {2, 4}, {5, 6}, {8, 10}, {12, 14}, {15, 17}}, 2, {{9, 7}, {11, 13}, {0, 0}}, {16, 18}},    // 8 E
+    {{{1, 3}, {2, 4}, {5, 6}, {7, 9}, {11, 13}, {15, 17}}, 2, {{10, 8}, {12, 14}, {0, 0}}, {16, 18}},    // 9 A
+    {{{3, 1}, {2, 4}, {5, 6}, {8, 10}, {12, 14}, {15, 17}}, 2, {{9, 7}, {11, 13}, {0, 0}}, {16, 18}},    // 10 B
+    {{{1, 3}, {2, 4}, {6, 5}, {7, 9}, {18, 16}, {14, 12}}, 2, {{10, 8}, {11, 13}, {0, 0}}, {15, 17}},    // 11 A'
+    {{{3, 1}, {2, 4}, {6, 5}, {8, 10}, {13, 11}, {18, 16}}, 2, {{9, 7}, {12, 14}, {0, 0}}, {15, 17}},    // 12 B'
+    {{{6, 5}, {7, 9}, {13, 11}, {14, 12}, {17, 15}, {18, 16}}, 3, {{1, 3}, {4, 2}, {8, 10}}, {-1, -1}},  // 13 D'
+    {{{6, 5}, {8, 10}, {13, 11}, {14, 12}, {17, 15}, {18, 16}}, 3, {{9, 7}, {4, 2}, {1, 3}}, {-1, -1}},  // 14 C'
+    {{{5, 6}, {8, 10}, {11, 13}, {12, 14}, {15, 17}, {16, 18}}, 3, {{1, 3}, {4, 2}, {9, 7}}, {-1, -1}},  // 15 C
+    {{{5, 6}, {7, 9}, {11, 13}, {12, 14}, {15, 17}, {16, 18}}, 3, {{1, 3}, {4, 2}, {8, 10}}, {-1, -1}},  // 16 D
+};
+
+// Corner closure on a local copy (runtime indices; 16 nodes per mixer).
+template <class PR>
+__device__ __forceinline__ void corner_closure(const BCtx<PR>& c, int fld, int n, typename PR::T R, typename PR::T* t)
+{
+    using T = typename PR::T;
+    const CornerSpec& s = kCorner[n];
+    for (int m = 0; m < 6; m++) t[s.bb[m][0]] = t[s.bb[m][1]];
+    T fa[3];
+    for (int m = 0; m < s.navg; m++) fa[m] = T(0.5) * (own_fn(c, fld, s.avg[m][0]) + own_fn(c, fld, s.avg[m][1]));
+    for (int m = 0; m < s.navg; m++) {
+        t[s.avg[m][0]] = fa[m];
+        t[s.avg[m][1]] = fa[m];
+    }
+    if (s.cp[0] >= 0) {
+        T sum = T(0);
+        bool first = true;
+        for (int q = 0; q < 19; q++) {
+            if (q == s.cp[0] || q == s.cp[1]) continue;
+            sum = first ? t[q] : sum + t[q];
+            first = false;
+        }
+        t[s.cp[0]] = T(0.5) * (R - sum);
+        t[s.cp[1]] = t[s.cp[0]];
+    }
+}
+
+// Apply the closure of class `cls` to field fld of the node in c, on v (the
+// node's pulled populations).  Closures follow the reference case by case;
+// the comments give the reference lines.  Face classes (inlets, outlet, walls)
+// and edge/corner classes are separate functions so that each boundary kernel
+// holds only the code of its own classes.
+template <class PR>
+__device__ __forceinline__ void closure_face(const BCtx<PR>& c, int cls, int fld, typename PR::T (&v)[19])
+{
+    using T = typename PR::T;
+    const bool flow = fld == 0;
+    switch (cls) {
+    case K_INLET1: {  // Inlet1 (:2606-2666)
+        if (flow) {
+            const T U = uin(c, 0, c.j, c.k);
+            const T r = (T(1) / (T(1) - U)) * ((v[0] + v[2] + v[4] + v[5] + v[6] + v[15] + v[16] + v[17] + v[18]) +
+                                                  T(2) * (v[3] + v[8] + v[9] + v[12] + v[13]));
+            const T A = (-r * U) / T(6);
+            const T B = T(0.5) * (v[2] - v[4] + v[15] - v[16] - v[17] + v[18]);
+            const T C = T(0.5) * (v[5] - v[6] + v[15] + v[16] - v[17] - v[18]);
+            v[1] = v[3] + (r * U) / T(3);
+            v[7] = v[9] - (A + B); v[10] = v[8] - (A - B); v[11] = v[13] - (A + C); v[14] = v[12] - (A - C);
+        } else {
+            const T cin = c.P->cin[fld - 1][0];
+            v[1] = -v[3] + T(2.0 / 18.0) * cin;
+            v[7] = -v[9] + T(2.0 / 36.0) * cin;
+            v[10] = -v[8] + T(2.0 / 36.0) * cin;
+            v[11] = -v[13] + T(2.0 / 36.0) * cin;
+            v[14] = -v[12] + T(2.0 / 36.0) * cin;
+        }
+    } break;
+    case K_INLET2: {  // Inlet2 (:2668-2730)
+        if (flow) {
+            const T U = uin(c, 1, c.j, c.k);
+            const T r = (T(1) / (T(1) + (U))) * ((v[0] + v[2] + v[4] + v[5] + v[6] + v[15] + v[16] + v[17] + v[18]) +
+                                                    T(2) * (v[1] + v[7] + v[10] + v[11] + v[14]));
+            const T A = (-r * (U)) / T(6);
+            const T B = T(0.5) * (v[2] - v[4] + v[15] - v[16] - v[17] + v[18]);
+            const T C = T(0.5) * (v[5] - v[6] + v[15] + v[16] - v[17] - v[18]);
+            v[3] = v[1] - (r * (U)) / T(3);
+            v[9] = v[7] + (A + B); v[8] = v[10] + (A - B); v[13] = v[11] + (A + C); v[12] = v[14] + (A - C);
+        } else {
+            const T cin = c.P->cin[fld - 1][1];
+            v[3] = -v[1] + T(2.0 / 18.0) * cin;
+            v[9] = -v[7] + T(2.0 / 36.0) * cin;
+            v[8] = -v[10] + T(2.0 / 36.0) * cin;
+            v[13] = -v[11] + T(2.0 / 36.0) * cin;
+            v[12] = -v[14] + T(2.0 / 36.0) * cin;
+        }
+    } break;
+    case K_FACE_YT: {  // Case 10 flow (:2731-2764); species copy from y-1 (:2766-2872)
+        if (flow) {
+            const T C = T(0.5) * (v[5] - v[6] + v[11] + v[12] - v[13] - v[14]);
+            v[4] = v[2]; v[16] = v[18] - C; v[17] = v[15] + C;
+            const T A = T(0.5) * (v[1] - v[3] + v[11] - v[12] - v[13] + v[14]);
+            v[9] = v[7] + A; v[10] = v[8] - A;
+        } else pull_node(c, fld, c.b, c.i, c.j - 1, c.k, v);
+    } break;
+    case K_FACE_Y1: {  // Cases 11, 12 flow (:2874-2906, :3016-3049); species copy from y+1
+        if (flow) {
+            const T C = T(0.5) * (v[5] - v[6] + v[11] + v[12] - v[13] - v[14]);
+            v[2] = v[4]; v[15] = v[17] - C; v[18] = v[16] + C;
+            const T A = T(0.5) * (v[1] - v[3] + v[11] - v[12] - v[13] + v[14]);
+            v[7] = v[9] - A; v[8] = v[10] + A;
+        } else pull_node(c, fld, c.b, c.i, c.j + 1, c.k, v);
+    } break;
+    case K_OUTLET: {  // Case 13 flow (:3162-3190); species copy from y+1 (:3192-3273)
+        if (flow) {
+            const T rout = c.P->rho_out;
+            const T uy = T(1) - (T(1) / rout) * ((v[0] + v[1] + v[3] + v[5] + v[6] + v[11] + v[12] + v[13] + v[14]) +
+                                                    T(2) * (v[4] + v[9] + v[10] + v[16] + v[17]));
+            const T A = (rout * uy) / T(6);
+            const T B = T(0.5) * ((v[3] + v[12] + v[13]) - (v[1] + v[11] + v[14]));
+            const T C = T(0.5) * ((v[6] + v[13] + v[14]) - (v[5] + v[11] + v[12]));
+            v[2] = v[4] + (rout * uy) / T(3);
+            v[7] = v[9] + (A + B); v[8] = v[10] + (A - B); v[15] = v[17] + (A + C); v[18] = v[16] + (A - C);
+        } else pull_node(c, fld, c.b, c.i, c.j + 1, c.k, v);
+    } break;
+    case K_FACE_MX1: {  // Case 14 (:3275-3404)
+        if (flow) {
+            const T C = T(0.5) * ((v[6] + v[17] + v[18]) - (v[5] + v[15] + v[16]));
+            v[1] = v[3]; v[11] = v[13] + (C); v[14] = v[12] - (C);
+            const T A = T(0.5) * ((v[2] + v[15] + v[18]) - (v[4] + v[16] + v[17]));
+            v[7] = v[9] - A; v[10] = v[8] + A;
+        } else pull_node(c, fld, c.b, c.i + 1, c.j, c.k, v);
+    } break;
+    case K_FACE_MXT: {  // Case 15 (:3405-3539)
+        if (flow) {
+            const T C = T(0.5) * ((v[6] + v[17] + v[18]) - (v[5] + v[15] + v[16]));
+            v[3] = v[1]; v[13] = v[11] - (C); v[12] = v[14] + (C);
+            const T A = T(0.5) * ((v[2] + v[15] + v[18]) - (v[4] + v[16] + v[17]));
+            v[9] = v[7] + A; v[8] = v[10] - A;
+        } else pull_node(c, fld, c.b, c.i - 1, c.j, c.k, v);
+    } break;
+    case K_FACE_ZT: {  // Cases 16, 17 and the opening nodes of 17 (:3540-3887)
+        if (flow) {
+            const T B = T(0.5) * (v[2] - v[4] + v[7] + v[8] - v[9] - v[10]);
+            v[6] = v[5]; v[17] = v[15] + B; v[18] = v[16] - B;
+            const T A = T(0.5) * (v[1] - v[3] + v[7] - v[8] - v[9] + v[10]);
+            v[13] = v[11] + A; v[14] = v[12] - A;
+        } else pull_node(c, fld, c.b, c.i, c.j, c.k - 1, v);
+    } break;
+    case K_FACE_Z1: {  // Cases 18, 19 and the opening nodes of 19 (:3888-4237)
+        if (flow) {
+            const T B = T(0.5) * (v[2] - v[4] + v[7] + v[8] - v[9] - v[10]);
+            v[5] = v[6]; v[15] = v[17] - B; v[16] = v[18] + B;
+            const T A = T(0.5) * (v[1] - v[3] + v[7] - v[8] - v[9] + v[10]);
+            v[11] = v[13] - A; v[12] = v[14] + A;
+        } else pull_node(c, fld, c.b, c.i, c.j, c.k + 1, v);
+    } break;
+    default: break;
+    }
+}
+
+template <class PR>
+__device__ __forceinline__ void closure_edge(const BCtx<PR>& c, int cls, int fld, typename PR::T (&v)[19])
+{
+    using T = typename PR::T;
+    const Geom& G = *c.G;
+    const bool flow = fld == 0;
+    switch (cls) {
+    case K_EDGE_Y1_ZTOP: {  // Cases 2, 3 (:2030-2342)
+        v[2] = v[4]; v[6] = v[5]; v[7] = v[9]; v[8] = v[10]; v[13] = v[11]; v[14] = v[12]; v[18] = v[16];
+        v[15] = T(0.5) * (own_fn(c, fld, 15) + own_fn(c, fld, 17));
+        v[17] = v[15];
+        const T A = T(0.25) * (v[1] - v[3]);
+        v[7] = v[9] - A; v[8] = v[10] + A; v[13] = v[11] + A; v[14] = v[12] - A;
+    } break;
+    case K_EDGE_X1_ZTOP: {  // Case 4 (:2343-2476); field C keeps p13 = pn13 (:2474)
+        const T B = T(0.25) * (v[2] - v[4]);
+        v[1] = v[3]; v[6] = v[5]; v[7] = v[9] - B; v[10] = v[8] + B; v[14] = v[12]; v[17] = v[15] + B; v[18] = v[16] - B;
+        v[13] = own_fn(c, fld, 13);
+        v[11] = T(0.5) * (rprev(c, fld, 0, 1, c.j, G.nz - 1) - sum_but(v, 11, 13));
+        if (fld != 3) v[13] = v[11];
+    } break;
+    case K_EDGE_XT_ZTOP: {  // Case 6 (:2477-2605)
+        const T B = T(0.25) * (v[2] - v[4]);
+        v[3] = v[1]; v[6] = v[5]; v[9] = v[7] + B; v[8] = v[10] - B; v[13] = v[11]; v[17] = v[15] + B; v[18] = v[16] - B;
+        v[12] = T(0.5) * (rprev(c, fld, 0, G.inx, c.j, G.nz - 1) - sum_but(v, 12, 14));
+        v[14] = v[12];
+    } break;
+    case K_EDGE_YT_ZT: {  // Case 20 (:4238-4385)
+        v[4] = v[2]; v[6] = v[5]; v[17] = v[15];
+        v[16] = T(0.5) * (own_fn(c, fld, 16) + own_fn(c, fld, 18));
+        v[18] = v[16];
+        const T A = T(0.25) * (v[1] - v[3]);
+        v[9] = v[7] + A; v[10] = v[8] - A; v[13] = v[11] + A; v[14] = v[12] - A;
+    } break;
+    case K_EDGE_YT_Z1: {  // Case 21 (:4386-4533)
+        v[4] = v[2]; v[5] = v[6]; v[16] = v[18];
+        v[15] = T(0.5) * (own_fn(c, fld, 15) + own_fn(c, fld, 17));
+        v[17] = v[15];
+        const T A = T(0.25) * (v[1] - v[3]);
+        v[9] = v[7] + A; v[10] = v[8] - A; v[11] = v[13] - A; v[12] = v[14] + A;
+    } break;
+    case K_EDGE_X1_Z1: {  // Case 22 (:4534-4656); flow density of (1,j,2) from this step
+        const T B = T(0.25) * (v[2] - v[4]);
+        v[1] = v[3]; v[5] = v[6]; v[7] = v[9] - B; v[10] = v[8] + B; v[11] = v[13]; v[15] = v[17] - B; v[16] = v[18] + B;
+        const T R = flow ? inlet_rho_now(c, 0, c.j, 2) : rprev(c, fld, 0, 1, c.j, 2);
+        v[12] = T(0.5) * (R - sum_but(v, 12, 14));
+        v[14] = v[12];
+    } break;
+    case K_EDGE_XT_Z1: {  // Case 23 (:4657-4779)
+        const T B = T(0.25) * (v[2] - v[4]);
+        v[3] = v[1]; v[5] = v[6]; v[8] = v[10] - B; v[9] = v[7] + B; v[12] = v[14]; v[15] = v[17] - B; v[16] = v[18] + B;
+        const T R = flow ? inlet_rho_now(c, 1, c.j, 2) : rprev(c, fld, 0, G.inx, c.j, 2);
+        v[11] = T(0.5) * (R - sum_but(v, 11, 13));
+        v[13] = v[11];
+    } break;
+    case K_EDGE_X1_Y1: {  // Case 24 (:4780-4909)
+        const T C = T(0.25) * (v[5] - v[6]);
+        v[1] = v[3]; v[2] = v[4]; v[7] = v[9]; v[11] = v[13] - C; v[14] = v[12] + C; v[15] = v[17] - C; v[18] = v[16] + C;
+        const T R = flow ? inlet_rho_now(c, 0, 2, c.k) : rprev(c, fld, 0, 1, 2, c.k);
+        v[8] = T(0.5) * (R - sum_but(v, 8, 10));
+        v[10] = v[8];
+    } break;
+    case K_EDGE_X1_YT: {  // Case 25 (:4910-5032)
+        const T C = T(0.25) * (v[5] - v[6]);
+        v[1] = v[3]; v[4] = v[2]; v[10] = v[8]; v[11] = v[13] - C; v[14] = v[12] + C; v[16] = v[18] - C; v[17] = v[15] + C;
+        const T R = flow ? inlet_rho_now(c, 0, G.iny - 1, c.k) : rprev(c, fld, 0, 1, G.iny - 1, c.k);
+        v[7] = T(0.5) * (R - sum_but(v, 7, 9));
+        v[9] = v[7];
+    } break;
+    case K_EDGE_XT_Y1: {  // Case 26 (:5033-5159)
+        const T C = T(0.25) * (v[5] - v[6]);
+        v[3] = v[1]; v[2] = v[4]; v[8] = v[10]; v[12] = v[14] - C; v[13] = v[11] + C; v[15] = v[17] - C; v[18] = v[16] + C;
+        const T R = flow ? inlet_rho_now(c, 1, 2, c.k) : rprev(c, fld, 0, G.inx, 2, c.k);
+        v[7] = T(0.5) * (R - sum_but(v, 7, 9));
+        v[9] = v[7];
+    } break;
+    case K_EDGE_XT_YT: {  // Case 27 (:5160-5281)
+        const T C = T(0.25) * (v[5] - v[6]);
+        v[3] = v[1]; v[4] = v[2]; v[9] = v[7]; v[12] = v[14] - C; v[13] = v[11] + C; v[16] = v[18] - C; v[17] = v[15] + C;
+        const T R = flow ? inlet_rho_now(c, 1, G.iny - 1, c.k) : rprev(c, fld, 0, G.inx, G.iny - 1, c.k);
+        v[8] = T(0.5) * (R - sum_but(v, 8, 10));
+        v[10] = v[8];
+    } break;
+    case K_EDGE_Y1_Z1: {  // Cases 28, 29 (:5282-5571)
+        v[2] = v[4]; v[5] = v[6]; v[15] = v[17];
+        v[16] = T(0.5) * (own_fn(c, fld, 16) + own_fn(c, fld, 18));
+        v[18] = v[16];
+        const T A = T(0.25) * (v[1] - v[3]);
+        v[7] = v[9] - A; v[8] = v[10] + A; v[11] = v[13] - A; v[12] = v[14] + A;
+    } break;
+    case K_MEDGE_AB: {  // (:7788-7868)
+        const T A = T(0.25) * (v[1] - v[3]);
+        v[2] = v[4]; v[5] = v[6]; v[7] = v[9] - A; v[8] = v[10] + A; v[11] = v[13] - A; v[12] = v[14] + A; v[15] = v[17];
+        const T R = flow ? T(c.P->rho_out) : rprev(c, fld, 1, c.i, 2, 1);
+        v[18] = T(0.5) * (R - sum_but(v, 16, 18));
+        v[16] = v[18];
+    } break;
+    case K_MEDGE_ApBp: {  // (:7870-7950)
+        const T A = T(0.25) * (v[1] - v[3]);
+        v[2] = v[4]; v[6] = v[5]; v[7] = v[9] - A; v[8] = v[10] + A; v[13] = v[11] + A; v[14] = v[12] - A; v[18] = v[16];
+        const T R = flow ? T(c.P->rho_out) : rprev(c, fld, 1, c.i, 2, G.nz);
+        v[15] = T(0.5) * (R - sum_but(v, 15, 17));
+        v[17] = v[15];
+    } break;
+    case K_MEDGE_AAp: {  // (:7951-8043)
+        const T C = T(0.25) * (v[5] - v[6]);
+        v[1] = v[3]; v[2] = v[4]; v[7] = v[9]; v[11] = v[13] - C; v[14] = v[12] + C; v[15] = v[17] - C; v[18] = v[16] + C;
+        const T R = flow ? T(c.P->rho_out) : rprev(c, fld, 1, 1, 2, c.k);
+        v[8] = T(0.5) * (R - sum_but(v, 8, 10));
+        v[10] = v[8];
+    } break;
+    case K_MEDGE_BBp: {  // (:8044-8136)
+        const T C = T(0.25) * (v[5] - v[6]);
+        v[3] = v[1]; v[2] = v[4]; v[8] = v[10]; v[12] = v[14] - C; v[13] = v[11] + C; v[15] = v[17] - C; v[18] = v[16] + C;
+        const T R = flow ? T(c.P->rho_out) : rprev(c, fld, 1, G.mnx, 2, c.k);
+        v[7] = T(0.5) * (R - sum_but(v, 7, 9));
+        v[9] = v[7];
+    } break;
+    case K_MEDGE_AD: {  // (:8137-8244)
+        const T B = T(0.25) * (v[2] - v[4]);
+        v[1] = v[3]; v[5] = v[6]; v[7] = v[9] - B; v[10] = v[8] + B; v[11] = v[13]; v[15] = v[17] - B; v[16] = v[18] + B;
+        v[14] = T(0.5) * (own_fn(c, fld, 12) + own_fn(c, fld, 14));
+        v[12] = v[14];
+    } break;
+    case K_MEDGE_ApDp: {  // (:8245-8344)
+        const T B = T(0.25) * (v[2] - v[4]);
+        v[1] = v[3]; v[6] = v[5]; v[7] = v[9] - B; v[10] = v[8] + B; v[14] = v[12]; v[17] = v[15] + B; v[18] = v[16] - B;
+        v[13] = T(0.5) * (own_fn(c, fld, 11) + own_fn(c, fld, 13));
+        v[11] = v[13];
+    } break;
+    case K_MEDGE_BC: {  // (:8345-8445)
+        const T B = T(0.25) * (v[2] - v[4]);
+        v[3] = v[1]; v[5] = v[6]; v[8] = v[10] - B; v[9] = v[7] + B; v[12] = v[14]; v[15] = v[17] - B; v[16] = v[18] + B;
+        v[13] = T(0.5) * (own_fn(c, fld, 11) + own_fn(c, fld, 13));
+        v[11] = v[13];
+    } break;
+    case K_MEDGE_BpCp: {  // (:8446-8550)
+        const T B = T(0.25) * (v[2] - v[4]);
+        v[3] = v[1]; v[6] = v[5]; v[9] = v[7] + B; v[8] = v[10] - B; v[13] = v[11]; v[17] = v[15] + B; v[18] = v[16] - B;
+        v[14] = T(0.5) * (own_fn(c, fld, 12) + own_fn(c, fld, 14));
+        v[12] = v[14];
+    } break;
+    case K_JUNC_DD:    // (:8551-8792): closed pair 7/9 from the density at (ia, 2, k)
+    case K_JUNC_CC: {  // (:8793-9033): closed pair 8/10 from the density at (ib, 2, k)
+        const bool dd = cls == K_JUNC_DD;
+        T a;
+        a = T(0.5) * (own_fn(c, fld, 3) + own_fn(c, fld, 1)); v[3] = a; v[1] = a;
+        a = T(0.5) * (own_fn(c, fld, 4) + own_fn(c, fld, 2)); v[4] = a; v[2] = a;
+        a = T(0.5) * (own_fn(c, fld, 5) + own_fn(c, fld, 6)); v[6] = a; v[5] = a;
+        a = T(0.5) * (own_fn(c, fld, 11) + own_fn(c, fld, 13)); v[13] = a; v[11] = a;
+        a = T(0.5) * (own_fn(c, fld, 12) + own_fn(c, fld, 14)); v[14] = a; v[12] = a;
+        a = T(0.5) * (own_fn(c, fld, 15) + own_fn(c, fld, 17)); v[17] = a; v[15] = a;
+        a = T(0.5) * (own_fn(c, fld, 16) + own_fn(c, fld, 18)); v[18] = a; v[16] = a;
+        const T R = rprev(c, fld, 0, dd ? G.ia : G.ib, 2, c.k);
+        if (dd) {
+            a = T(0.5) * (own_fn(c, fld, 8) + own_fn(c, fld, 10)); v[10] = a; v[8] = a;
+            v[7] = T(0.5) * (R - sum_but(v, 7, 9));
+            v[9] = v[7];
+        } else {
+            a = T(0.5) * (own_fn(c, fld, 7) + own_fn(c, fld, 9)); v[9] = a; v[7] = a;
+            v[8] = T(0.5) * (R - sum_but(v, 8, 10));
+            v[10] = v[8];
+        }
+    } break;
+    default: {
+        if (cls >= K_CORNER_1 && cls <= K_CORNER_16) {
+            const int n = cls - K_CORNER_1;
+            T R = T(0);
+            if (n < 8) {  // inlet corners: density of the adjacent x-y edge node
+                R = rprev(c, fld, 0, c.i, c.j, c.k == G.nz ? G.nz - 1 : 2);
+            } else if (n < 12) {  // outlet corners: rho_out; species read the row
+                R = flow ? T(c.P->rho_out) : T(0);  // below the outlet, which is 0
+            }
+            T t[19];
+#pragma unroll
+            for (int q = 0; q < 19; q++) t[q] = v[q];
+            corner_closure(c, fld, n, R, t);
+#pragma unroll
+            for (int q = 0; q < 19; q++) v[q] = t[q];
+        }
+    } break;
+    }
+}
+
+// The post-closure populations of field fld of the boundary node in c.  A
+// species on a wall face is a zero-gradient copy of an interior node's pulled
+// populations (Tmixer.cpp:2766-4237), so it pulls that node directly.
+template <class PR, bool FACES>
+__device__ __forceinline__ void closed_pull(const BCtx<PR>& c, int cls, int fld, typename PR::T (&v)[19])
+{
+    if (FACES && fld > 0) {
+        int di = 0, dj = 0, dk = 0;
+        switch (cls) {
+        case K_FACE_YT: dj = -1; break;
+        case K_FACE_Y1:
+        case K_OUTLET: dj = 1; break;
+        case K_FACE_MX1: di = 1; break;
+        case K_FACE_MXT: di = -1; break;
+        case K_FACE_ZT: dk = -1; break;
+        case K_FACE_Z1: dk = 1; break;
+        default: break;
+        }
+        if (di | dj | dk) {
+            pull_node(c, fld, c.b, c.i + di, c.j + dj, c.k + dk, v);
+            return;
+        }
+    }
+    pull_node(c, fld, c.b, c.i, c.j, c.k, v);
+    if (FACES)
+        closure_face(c, cls, fld, v);
+    else
+        closure_edge(c, cls, fld, v);
+}
+
+// ---------------------------------------------------------------------------
+// boundary nodes: one thread per node of a compact, class-sorted list; FACES
+// selects the list of inlet/outlet/wall-face nodes or of edge/corner nodes.
+// The closed species A and B populations wait in shared memory while the
+// reaction term (which needs both densities) is formed.
+// ---------------------------------------------------------------------------
+constexpr int kBoundaryThreads = 128;
+
+template <class PR, bool FACES>
+__device__ __forceinline__ void boundary_node(const typename PR::S* __restrict__ Pin,
+                                              typename PR::S* __restrict__ Pout,
+                                              const typename PR::T* __restrict__ Rprev,
+                                              typename PR::T* __restrict__ Rcur, double* __restrict__ Mac,
+                                              const int* __restrict__ bnode, const unsigned char* __restrict__ bcls,
+                                              int nb, const typename PR::T* __restrict__ uin1,
+                                              const typename PR::T* __restrict__ uin2, const Geom& G, const Phys& P,
+                                              int write_macro, typename PR::T (*stash)[19][kBoundaryThreads])
+{
+    using T = typename PR::T;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nb) return;
+    BCtx<PR> c;
+    c.Pin = Pin;
+    c.Rprev = Rprev;
+    c.uin1 = uin1;
+    c.uin2 = uin2;
+    c.G = &G;
+    c.P = &P;
+    c.ps = G.ps;
+    c.g = bnode[t];
+    decode(G, c.g, c.b, c.i, c.j, c.k);
+    const int cls = bcls[t];
+    const long long ps = G.ps;
+    const bool outlet = c.b == 1 && c.j == 1;
+    const int tx = threadIdx.x;
+
+    T poly[19];
+    T rho, ux, uy, uz;
+    {
+        T f[19];
+        closed_pull<PR, FACES>(c, cls, 0, f);
+        // the outlet row's density is pinned to rho_out (Tmixer.cpp:9575-9582)
+        rho = outlet ? T(P.rho_out) : sum19(f);
+        T sxm, sym, szm;
+        momentum(f, sxm, sym, szm);
+        ux = sxm / rho;
+        uy = sym / rho;
+        uz = szm / rho;
+        eq_poly(ux, uy, uz, poly);
+        collide_store<PR>(Pout, ps, c.g, 0, f, rho, poly, P, T(0));
+    }
+    T ca, cb, cc;
+    {
+        T v[19];
+        closed_pull<PR, FACES>(c, cls, 1, v);
+        ca = sum19(v);
+#pragma unroll
+        for (int q = 0; q < 19; q++) stash[0][q][tx] = v[q];
+        closed_pull<PR, FACES>(c, cls, 2, v);
+        cb = sum19(v);
+#pragma unroll
+        for (int q = 0; q < 19; q++) stash[1][q][tx] = v[q];
+    }
+    const T rt = T(P.rateconst) * ca * cb;
+    {
+        T v[19];
+#pragma unroll
+        for (int q = 0; q < 19; q++) v[q] = stash[0][q][tx];
+        collide_store<PR>(Pout, ps, c.g, 1, v, ca, poly, P, rt);
+#pragma unroll
+        for (int q = 0; q < 19; q++) v[q] = stash[1][q][tx];
+        collide_store<PR>(Pout, ps, c.g, 2, v, cb, poly, P, rt);
+        closed_pull<PR, FACES>(c, cls, 3, v);
+        cc = sum19(v);
+        collide_store<PR>(Pout, ps, c.g, 3, v, cc, poly, P, rt);
+    }
+
+    Rcur[c.g] = rho;
+    Rcur[ps + c.g] = ca;
+    Rcur[2 * ps + c.g] = cb;
+    Rcur[3 * ps + c.g] = cc;
+    if (write_macro) {
+        Mac[c.g] = rho;
+        Mac[ps + c.g] = ux;
+        Mac[2 * ps + c.g] = uy;
+        Mac[3 * ps + c.g] = uz;
+        Mac[4 * ps + c.g] = ca;
+        Mac[5 * ps + c.g] = cb;
+        Mac[6 * ps + c.g] = cc;
+    }
+}
+
+// Kernel definitions for one precision policy; NAME is the kernel-name suffix.
+#define TMX_DEFINE_STEP_KERNELS(PR, NAME)                                                                         \
+    __global__ void k_init_##NAME(void* Pout, void* R, double* Mac, Geom G, Phys P, double rho0)                \
+    {                                                                                                           \
+        for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < G.nnodes; g += gridDim.x * blockDim.x)          \
+            init_node<PR>((PR::S*)Pout, (PR::T*)R, Mac, G, P, rho0, g);                                         \
+    }                                                                                                           \
+    __global__ void __launch_bounds__(256, 2)                                                                   \
+        k_bulk_##NAME(const void* Pin, void* Pout, void* Rcur, double* Mac, Geom G, Phys P, int write_macro)    \
+    {                                                                                                           \
+        for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < G.nnodes; g += gridDim.x * blockDim.x)          \
+            bulk_node<PR>((const PR::S*)Pin, (PR::S*)Pout, (PR::T*)Rcur, Mac, G, P, write_macro, g);            \
+    }                                                                                                           \
+    __global__ void __launch_bounds__(kBoundaryThreads)                                                        \
+        k_bfaces_##NAME(const void* Pin, void* Pout, const void* Rprev, void* Rcur, double* Mac,                \
+                        const int* bnode, const unsigned char* bcls, int nb, const void* uin1, const void* uin2, \
+                        Geom G, Phys P, int write_macro)                                                        \
+    {                                                                                                           \
+        __shared__ PR::T stash[2][19][kBoundaryThreads];                                                        \
+        boundary_node<PR, true>((const PR::S*)Pin, (PR::S*)Pout, (const PR::T*)Rprev, (PR::T*)Rcur, Mac, bnode, \
+                                bcls, nb, (const PR::T*)uin1, (const PR::T*)uin2, G, P, write_macro, stash);    \
+    }                                                                                                           \
+    __global__ void __launch_bounds__(kBoundaryThreads)                                                        \
+        k_bedges_##NAME(const void* Pin, void* Pout, const void* Rprev, void* Rcur, double* Mac,                \
+                        const int* bnode, const unsigned char* bcls, int nb, const void* uin1, const void* uin2, \
+                        Geom G, Phys P, int write_macro)                                                        \
+    {                                                                                                           \
+        __shared__ PR::T stash[2][19][kBoundaryThreads];                                                        \
+        boundary_node<PR, false>((const PR::S*)Pin, (PR::S*)Pout, (const PR::T*)Rprev, (PR::T*)Rcur, Mac,       \
+                                 bnode, bcls, nb, (const PR::T*)uin1, (const PR::T*)uin2, G, P, write_macro,    \
+                                 stash);                                                                        \
+    }
+
+}  // namespace tmx

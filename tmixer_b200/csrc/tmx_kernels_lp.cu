@@ -1,0 +1,13 @@
+// tmx_kernels_lp.cu -- sm_100a kernels of the reduced-precision forms: FP32
+// arithmetic with FP32 storage, and FP32 arithmetic with populations stored in
+// FP16 as f_q - w_q*ref (the deviation from a reference density).  Compiled
+// with multiply-add contraction (the default); results are compared with the
+// FP64 form within stated tolerances, not bit for bit.
+#include "tmx_engine.cuh"
+
+namespace tmx {
+
+TMX_DEFINE_STEP_KERNELS(F32, f32)
+TMX_DEFINE_STEP_KERNELS(F16, f16)
+
+}  // namespace tmx
