@@ -42,7 +42,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
     headers.append(os.path.join(ROOT, "include", "tmx.h"))
     os.makedirs(OBJDIR, exist_ok=True)
-    objs = []
+    objs, jobs = [], []
     for src, flags in SOURCES.items():
         path = os.path.join(CSRC, src)
         obj = os.path.join(OBJDIR, src + ".o")
@@ -51,7 +51,10 @@ def build(force: bool = False, verbose: bool = False) -> str:
             cmd = [_nvcc()] + NVCC_FLAGS + flags + ARCH + ["-c", "-o", obj, path]
             if verbose:
                 print(" ".join(cmd), file=sys.stderr)
-            subprocess.run(cmd, check=True)
+            jobs.append((cmd, subprocess.Popen(cmd)))
+    for cmd, proc in jobs:
+        if proc.wait() != 0:
+            raise subprocess.CalledProcessError(proc.returncode, cmd)
     if force or _stale(LIB, objs):
         tmp = LIB + ".tmp"
         cmd = [_nvcc()] + ARCH + ["-shared", "-o", tmp] + objs

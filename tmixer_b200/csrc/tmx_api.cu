@@ -59,6 +59,7 @@ struct tmx_handle {
     unsigned char* bcls = nullptr;
     int nb = 0;
     void* uin_d[2] = {nullptr, nullptr};
+    float4* mom[2] = {nullptr, nullptr};  // FP16 form: moments of the nodes that wrote pop[s]
     double* stats = nullptr;
     double* partial = nullptr;
     std::vector<double> uin1, uin2;
@@ -82,23 +83,35 @@ struct tmx_handle {
 
 // the step kernels of one form
 struct StepKernels {
-    void (*init)(void*, void*, double*, Geom, Phys, double);
-    void (*bulk)(const void*, void*, void*, double*, Geom, Phys, int);
-    void (*faces)(const void*, void*, const void*, void*, double*, const int*, const unsigned char*, int, const void*,
-                  const void*, Geom, Phys, int);
-    void (*edges)(const void*, void*, const void*, void*, double*, const int*, const unsigned char*, int, const void*,
-                  const void*, Geom, Phys, int);
+    void (*init)(tmx::StepPtrs, Geom, Phys, double);
+    void (*bulk)(tmx::StepPtrs, Geom, Phys, int);
+    void (*faces)(tmx::StepPtrs, const int*, const unsigned char*, int, Geom, Phys, int);
+    void (*edges)(tmx::StepPtrs, const int*, const unsigned char*, int, Geom, Phys, int);
     int sbytes, tbytes;
+    bool moments;  // the form stores per-node FP32 moments next to the populations
 };
 static const StepKernels kForms[3] = {
-    {tmx::k_init_f64, tmx::k_bulk_f64, tmx::k_bfaces_f64, tmx::k_bedges_f64, 8, 8},
-    {tmx::k_init_f32, tmx::k_bulk_f32, tmx::k_bfaces_f32, tmx::k_bedges_f32, 4, 4},
-    {tmx::k_init_f16, tmx::k_bulk_f16, tmx::k_bfaces_f16, tmx::k_bedges_f16, 2, 4},
+    {tmx::k_init_f64, tmx::k_bulk_f64, tmx::k_bfaces_f64, tmx::k_bedges_f64, 8, 8, false},
+    {tmx::k_init_f32, tmx::k_bulk_f32, tmx::k_bfaces_f32, tmx::k_bedges_f32, 4, 4, false},
+    {tmx::k_init_f16, tmx::k_bulk_f16, tmx::k_bfaces_f16, tmx::k_bedges_f16, 2, 4, true},
 };
 
 namespace {
 
 constexpr int kSumBlocks = 592;
+
+// The FP16 form's equilibrium polynomial (tmx_engine.cuh poly_q_rn), in host
+// single precision with every operation rounded on its own.
+float poly_q_host(int q, float ux, float uy, float uz)
+{
+    const int ex = tmx::EX(q), ey = tmx::EY(q), ez = tmx::EZ(q);
+    const float u2 = (ux * ux + uy * uy) + uz * uz;
+    const float t = 1.5f * u2;
+    if (q == 0) return 1.0f - t;
+    const float a = ex > 0 ? ux : -ux, b = ey > 0 ? uy : -uy, c = ez > 0 ? uz : -uz;
+    const float eu = ex ? (ey ? a + b : (ez ? a + c : a)) : (ey ? (ez ? b + c : b) : c);
+    return ((1.0f + 3.0f * eu) - t) + (4.5f * eu) * eu;
+}
 
 // IEEE binary16 bits to float (host side of tmx_populations)
 float half_bits_to_float(unsigned short h)
@@ -139,9 +152,6 @@ void physics_of(const tmx_case& c, Phys& P)
     }
     P.rateconst = c.rateconst;
     P.rho_out = c.rho_out;
-    // reduced-precision storage keeps f_q - w_q*rho0 for the flow; species unshifted
-    P.ref[0] = c.rho0;
-    P.ref[1] = P.ref[2] = P.ref[3] = 0.0;
     for (int s = 0; s < 3; s++)
         for (int n = 0; n < 2; n++) P.cin[s][n] = c.c_in[s][n];
 }
@@ -152,6 +162,7 @@ long long footprint(const Geom& G, long long nb, int precision)
     long long b = 0;
     b += 2LL * 76 * G.ps * K.sbytes;  // populations
     b += 2LL * 4 * G.ps * K.tbytes;   // densities
+    if (K.moments) b += 2LL * 2 * G.ps * 16;  // FP16 form: moments
     b += 7LL * G.ps * 8;       // macroscopic fields
     b += nb * 5;               // boundary list
     b += 2LL * (G.iny + 3) * (G.nz + 3) * K.tbytes;
@@ -269,7 +280,9 @@ void free_all(tmx_handle* h)
         cudaFree(h->pop[s]);
         cudaFree(h->rho[s]);
         cudaFree(h->uin_d[s]);
+        cudaFree(h->mom[s]);
         h->pop[s] = h->rho[s] = h->uin_d[s] = nullptr;
+        h->mom[s] = nullptr;
     }
     for (int a = 0; a < 2; a++)
         for (int m = 0; m < 2; m++)
@@ -304,10 +317,16 @@ void free_all(tmx_handle* h)
 int enqueue_step(tmx_handle* h, int cur, int write_macro, cudaEvent_t* ev)
 {
     const Geom& G = h->G;
-    const void* pin = h->pop[cur];
-    void* pout = h->pop[1 - cur];
-    const void* rprev = h->rho[cur];
-    void* rcur = h->rho[1 - cur];
+    tmx::StepPtrs X;
+    X.pin = h->pop[cur];
+    X.pout = h->pop[1 - cur];
+    X.rprev = h->rho[cur];
+    X.rcur = h->rho[1 - cur];
+    X.mac = h->mac;
+    X.mprev = h->mom[cur];
+    X.mcur = h->mom[1 - cur];
+    X.uin1 = h->uin_d[0];
+    X.uin2 = h->uin_d[1];
     TMX_CK(cudaEventRecord(h->fork, h->stream));
     TMX_CK(cudaStreamWaitEvent(h->aux, h->fork, 0));
     TMX_CK(cudaStreamWaitEvent(h->aux2, h->fork, 0));
@@ -315,13 +334,10 @@ int enqueue_step(tmx_handle* h, int cur, int write_macro, cudaEvent_t* ev)
     const int nf = h->nface, ne = h->nb - h->nface;
     const int bt = tmx::kBoundaryThreadsHost;
     if (nf > 0)
-        h->K->faces<<<(nf + bt - 1) / bt, bt, 0, h->aux>>>(pin, pout, rprev, rcur, h->mac, h->bnode,
-                                                                   h->bcls, nf, h->uin_d[0], h->uin_d[1], G, h->P,
-                                                                   write_macro);
+        h->K->faces<<<(nf + bt - 1) / bt, bt, 0, h->aux>>>(X, h->bnode, h->bcls, nf, G, h->P, write_macro);
     if (ne > 0)
-        h->K->edges<<<(ne + bt - 1) / bt, bt, 0, h->aux2>>>(pin, pout, rprev, rcur, h->mac,
-                                                                     h->bnode + nf, h->bcls + nf, ne, h->uin_d[0],
-                                                                     h->uin_d[1], G, h->P, write_macro);
+        h->K->edges<<<(ne + bt - 1) / bt, bt, 0, h->aux2>>>(X, h->bnode + nf, h->bcls + nf, ne, G, h->P,
+                                                            write_macro);
     TMX_CK(cudaEventRecord(h->join2, h->aux2));
     if (ev) {  // the boundary time spans both boundary kernels
         TMX_CK(cudaStreamWaitEvent(h->aux, h->join2, 0));
@@ -329,7 +345,7 @@ int enqueue_step(tmx_handle* h, int cur, int write_macro, cudaEvent_t* ev)
     }
     TMX_CK(cudaEventRecord(h->join, h->aux));
     if (ev) TMX_CK(cudaEventRecord(ev[0], h->stream));
-    h->K->bulk<<<h->bulk_blocks, 256, 0, h->stream>>>(pin, pout, rcur, h->mac, G, h->P, write_macro);
+    h->K->bulk<<<h->bulk_blocks, 256, 0, h->stream>>>(X, G, h->P, write_macro);
     if (ev) TMX_CK(cudaEventRecord(ev[1], h->stream));
     TMX_CK(cudaStreamWaitEvent(h->stream, h->join, 0));
     TMX_CK(cudaStreamWaitEvent(h->stream, h->join2, 0));
@@ -535,6 +551,7 @@ int tmx_create(const tmx_case* c, int device, tmx_handle** out)
         e = alloc((void**)&h->pop[s], (size_t)76 * G.ps * h->sbytes);
         if (e == cudaSuccess) e = alloc((void**)&h->rho[s], (size_t)4 * G.ps * h->tbytes);
         if (e == cudaSuccess) e = alloc((void**)&h->uin_d[s], (size_t)(G.iny + 3) * (G.nz + 3) * h->tbytes);
+        if (e == cudaSuccess && h->K->moments) e = alloc((void**)&h->mom[s], (size_t)2 * G.ps * sizeof(float4));
     }
     if (e == cudaSuccess) e = alloc((void**)&h->mac, (size_t)7 * G.ps * sizeof(double));
     if (e == cudaSuccess) e = alloc((void**)&h->bnode, std::max<size_t>(1, nodes.size()) * sizeof(int));
@@ -574,7 +591,12 @@ int tmx_init(tmx_handle* h)
     }
     h->cur = 0;
     h->rcur = 0;
-    h->K->init<<<h->bulk_blocks, 256, 0, h->stream>>>(h->pop[0], h->rho[0], h->mac, h->G, h->P, h->c.rho0);
+    tmx::StepPtrs X{};
+    X.pout = h->pop[0];
+    X.rcur = h->rho[0];
+    X.mac = h->mac;
+    X.mcur = h->mom[0];
+    h->K->init<<<h->bulk_blocks, 256, 0, h->stream>>>(X, h->G, h->P, h->c.rho0);
     TMX_CK(cudaGetLastError());
     TMX_CK(cudaStreamSynchronize(h->stream));
     h->steps = 0;
@@ -650,14 +672,21 @@ int tmx_populations(tmx_handle* h, int box, int fld, double* host_out)
         }
         return TMX_OK;
     }
-    // reduced precision: widen (and add back the storage shift) on the host
+    // reduced precision: widen on the host; the FP16 form adds back feq of
+    // the writing node's moments exactly as the kernels do (tmx_engine.cuh)
     std::vector<double> wide(n);
     std::vector<unsigned char> raw(n * h->sbytes);
-    const double w[3] = {1.0 / 3.0, 1.0 / 18.0, 1.0 / 36.0};
+    std::vector<float> mf(4 * n), ms(4 * n);
+    if (h->K->moments) {
+        const float4* m = h->mom[h->cur];
+        TMX_CK(cudaMemcpy(mf.data(), m + G.base[box], n * sizeof(float4), cudaMemcpyDeviceToHost));
+        TMX_CK(cudaMemcpy(ms.data(), m + G.ps + G.base[box], n * sizeof(float4), cudaMemcpyDeviceToHost));
+    }
     for (int q = 0; q < 19; q++) {
-        const unsigned char* src = (const unsigned char*)h->pop[h->cur] + ((size_t)(fld * 19 + q) * G.ps + G.base[box]) * h->sbytes;
+        const unsigned char* src =
+            (const unsigned char*)h->pop[h->cur] + ((size_t)(fld * 19 + q) * G.ps + G.base[box]) * h->sbytes;
         TMX_CK(cudaMemcpy(raw.data(), src, raw.size(), cudaMemcpyDeviceToHost));
-        const float sh = (float)(q == 0 ? w[0] : (q <= 6 ? w[1] : w[2])) * (float)h->P.ref[fld];
+        const float w = (float)(q == 0 ? 1.0 / 3.0 : (q <= 6 ? 1.0 / 18.0 : 1.0 / 36.0));
         for (size_t t = 0; t < n; t++) {
             float v;
             if (h->sbytes == 4) {
@@ -665,7 +694,8 @@ int tmx_populations(tmx_handle* h, int box, int fld, double* host_out)
             } else {
                 unsigned short hb;
                 std::memcpy(&hb, &raw[t * 2], 2);
-                v = half_bits_to_float(hb) + sh;
+                const float r = fld == 0 ? mf[4 * t] : ms[4 * t + fld - 1];
+                v = half_bits_to_float(hb) + (r * poly_q_host(q, mf[4 * t + 1], mf[4 * t + 2], mf[4 * t + 3])) * w;
             }
             wide[t] = v;
         }

@@ -46,7 +46,6 @@ struct Phys {
     double rateconst;
     double rho_out;
     double cin[3][2];
-    double ref[4];  // storage shift of the reduced-precision forms: f_q is kept as f_q - w_q*ref[field]
 };
 
 __host__ __device__ inline bool is_boundary(const Geom& G, int b, int i, int j, int k)

@@ -31,6 +31,7 @@
 
 #include "tmx_classes.h"
 #include "tmx_device.cuh"
+#include "tmx_kernels.cuh"
 
 namespace tmx {
 
@@ -38,41 +39,77 @@ namespace tmx {
 // precision policies
 // ---------------------------------------------------------------------------
 
+// Deterministic FP32 equilibrium polynomial (every operation rounded on its
+// own, no contraction): the FP16 form adds and subtracts this value when it
+// encodes and decodes populations, so both sides must produce the same bits.
+__device__ __forceinline__ float poly_q_rn(int q, float ux, float uy, float uz)
+{
+    const float u2 = __fadd_rn(__fadd_rn(__fmul_rn(ux, ux), __fmul_rn(uy, uy)), __fmul_rn(uz, uz));
+    const float t = __fmul_rn(1.5f, u2);
+    if (q == 0) return __fsub_rn(1.0f, t);
+    const float eu = e_dot_u(q, ux, uy, uz);
+    return __fadd_rn(__fsub_rn(__fadd_rn(1.0f, __fmul_rn(3.0f, eu)), t), __fmul_rn(__fmul_rn(4.5f, eu), eu));
+}
+
 // Plain form: FP64 storage and arithmetic, operation by operation as the
 // reference (the translation unit is compiled with --fmad=false); the
 // equilibrium divisions are correctly rounded (div_c).
 struct F64 {
     using T = double;
     using S = double;
-    __device__ static T load(const S* p, T) { return __ldg(p); }
-    __device__ static void store(S* p, T v, T) { *p = v; }
-    __device__ static T shift(int, int, const Phys&) { return 0.0; }
+    static constexpr bool kMoments = false;
+    __device__ static void poly(T ux, T uy, T uz, T (&p)[19]) { eq_poly(ux, uy, uz, p); }
     __device__ static bool tiny(T r) { return tiny_density(r); }
-    __device__ static T feq(T x, int q, bool tiny) { return tiny ? feq_div_exact(x, q) : feq_div(x, q); }
+    __device__ static T feq(T r, T polyq, int q, bool tiny)
+    {
+        const T x = r * polyq;
+        return tiny ? feq_div_exact(x, q) : feq_div(x, q);
+    }
+    __device__ static T decode(const S* p, int, int, const float4*, long long, int) { return __ldg(p); }
+    __device__ static void encode(S* p, T v, T) { *p = v; }
 };
 
-// FP32 arithmetic and storage (no shift).
+// FP32 arithmetic and storage.
 struct F32 {
     using T = float;
     using S = float;
-    __device__ static T load(const S* p, T) { return __ldg(p); }
-    __device__ static void store(S* p, T v, T) { *p = v; }
-    __device__ static T shift(int, int, const Phys&) { return 0.0f; }
+    static constexpr bool kMoments = false;
+    __device__ static void poly(T ux, T uy, T uz, T (&p)[19]) { eq_poly(ux, uy, uz, p); }
     __device__ static bool tiny(T) { return false; }
-    __device__ static T feq(T x, int q, bool) { return x * (float)wq(q); }
+    __device__ static T feq(T r, T polyq, int q, bool) { return r * polyq * (float)wq(q); }
+    __device__ static T decode(const S* p, int, int, const float4*, long long, int) { return __ldg(p); }
+    __device__ static void encode(S* p, T v, T) { *p = v; }
 };
 
-// FP32 arithmetic on populations stored in FP16 as f_q - w_q*ref[field]
-// (ref = rho0 for the flow, so only the deviation from rest is stored).
+// FP32 arithmetic; populations stored in FP16 as their non-equilibrium part
+// n_q = f_q - feq_q(rho, u) of the node that wrote them, next to that node's
+// FP32 moments M = {(rho, ux, uy, uz), (cA, cB, cC, 0)} (float4[2*ps]).  A
+// reader adds back feq_q of the writer's moments.  The stored quantity is of
+// the order of the gradients, so FP16 keeps about FP32 accuracy of f.
 struct F16 {
     using T = float;
     using S = __half;
-    __device__ static T load(const S* p, T sh) { return __half2float(__ldg(p)) + sh; }
-    __device__ static void store(S* p, T v, T sh) { *p = __float2half_rn(v - sh); }
-    __device__ static T shift(int fld, int q, const Phys& P) { return (float)wq(q) * (float)P.ref[fld]; }
+    static constexpr bool kMoments = true;
+    __device__ static void poly(T ux, T uy, T uz, T (&p)[19])
+    {
+#pragma unroll
+        for (int q = 0; q < 19; q++) p[q] = poly_q_rn(q, ux, uy, uz);
+    }
     __device__ static bool tiny(T) { return false; }
-    __device__ static T feq(T x, int q, bool) { return x * (float)wq(q); }
+    __device__ static T feq(T r, T polyq, int q, bool) { return __fmul_rn(__fmul_rn(r, polyq), (float)wq(q)); }
+    __device__ static T decode(const S* p, int fld, int q, const float4* M, long long ps, int src)
+    {
+        const float4 mf = __ldg(M + src);
+        float r = mf.x;
+        if (fld > 0) {
+            const float4 ms = __ldg(M + ps + src);
+            r = fld == 1 ? ms.x : (fld == 2 ? ms.y : ms.z);
+        }
+        return __half2float(__ldg(p)) + feq(r, poly_q_rn(q, mf.y, mf.z, mf.w), q, false);
+    }
+    __device__ static void encode(S* p, T v, T feq) { *p = __float2half_rn(v - feq); }
 };
+
 
 // ---------------------------------------------------------------------------
 // per-node physics: equilibrium -> collision -> store
@@ -94,11 +131,11 @@ __device__ __forceinline__ void collide_store(typename PR::S* __restrict__ Pout,
     const bool tiny = PR::tiny(r);
 #pragma unroll
     for (int q = 0; q < 19; q++) {
-        const T feq = PR::feq(r * poly[q], q, tiny);
+        const T feq = PR::feq(r, poly[q], q, tiny);
         T v = f[q] * c1 + c2 * feq;
         if (fld == 1 || fld == 2) v = v - T(wq(q)) * rt;
         if (fld == 3) v = v + (T(wq(q)) * rt) * T(2);
-        PR::store(out + (long long)q * ps, v, PR::shift(fld, q, P));
+        PR::encode(out + (long long)q * ps, v, feq);
     }
 }
 
@@ -106,15 +143,19 @@ __device__ __forceinline__ void collide_store(typename PR::S* __restrict__ Pout,
 // initial state: f = feq(rho0, 0) for the flow and 0 for the species
 // (Tmixer.cpp:1544-1585, 1835-2018), then the first step's collision.
 // ---------------------------------------------------------------------------
+// Writes the state the first step reads: populations to X.pout, densities to
+// X.rcur, moments (FP16 form) to X.mcur.
 template <class PR>
-__device__ __forceinline__ void init_node(typename PR::S* __restrict__ Pout, typename PR::T* __restrict__ R,
-                                          double* __restrict__ Mac, const Geom& G, const Phys& P, double rho0d, int g)
+__device__ __forceinline__ void init_node(const StepPtrs& X, const Geom& G, const Phys& P, double rho0d, int g)
 {
     using T = typename PR::T;
+    typename PR::S* Pout = (typename PR::S*)X.pout;
+    T* R = (T*)X.rcur;
+    double* Mac = X.mac;
     const long long ps = G.ps;
     const T rho0 = T(rho0d);
     T poly[19];
-    eq_poly(T(0), T(0), T(0), poly);
+    PR::poly(T(0), T(0), T(0), poly);
     T f[19], z[19];
 #pragma unroll
     for (int q = 0; q < 19; q++) {
@@ -134,6 +175,10 @@ __device__ __forceinline__ void init_node(typename PR::S* __restrict__ Pout, typ
     Mac[g] = rho0d;
 #pragma unroll
     for (int m = 1; m < 7; m++) Mac[m * ps + g] = 0.0;
+    if (PR::kMoments) {
+        X.mcur[g] = make_float4((float)rho0, 0.f, 0.f, 0.f);
+        X.mcur[ps + g] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -152,24 +197,27 @@ __device__ __forceinline__ int bulk_src(const Geom& G, int g, int i, int k, int 
 }
 
 template <class PR>
-__device__ __forceinline__ void bulk_load(const typename PR::S* __restrict__ Pin, long long ps, int fld,
-                                          const Geom& G, const Phys& P, int g, int i, int k, int sy, int sz,
+__device__ __forceinline__ void bulk_load(const typename PR::S* __restrict__ Pin, const float4* __restrict__ M,
+                                          long long ps, int fld, const Geom& G, int g, int i, int k, int sy, int sz,
                                           int iface, typename PR::T (&v)[19])
 {
     const typename PR::S* base = Pin + (long long)fld * 19 * ps;
 #pragma unroll
-    for (int q = 0; q < 19; q++)
-        v[q] = PR::load(base + (long long)q * ps + bulk_src(G, g, i, k, sy, sz, iface, q), PR::shift(fld, q, P));
+    for (int q = 0; q < 19; q++) {
+        const int src = bulk_src(G, g, i, k, sy, sz, iface, q);
+        v[q] = PR::decode(base + (long long)q * ps + src, fld, q, M, ps, src);
+    }
 }
 
 // One interior node; returns false for a boundary node (left to the boundary
 // kernels).
 template <class PR>
-__device__ __forceinline__ void bulk_node(const typename PR::S* __restrict__ Pin, typename PR::S* __restrict__ Pout,
-                                          typename PR::T* __restrict__ Rcur, double* __restrict__ Mac, const Geom& G,
-                                          const Phys& P, int write_macro, int g)
+__device__ __forceinline__ void bulk_node(const StepPtrs& X, const Geom& G, const Phys& P, int write_macro, int g)
 {
     using T = typename PR::T;
+    const typename PR::S* __restrict__ Pin = (const typename PR::S*)X.pin;
+    typename PR::S* __restrict__ Pout = (typename PR::S*)X.pout;
+    const float4* __restrict__ M = X.mprev;
     const long long ps = G.ps;
     int b, i, j, k;
     decode(G, g, b, i, j, k);
@@ -183,14 +231,14 @@ __device__ __forceinline__ void bulk_node(const typename PR::S* __restrict__ Pin
     T rho, ux, uy, uz;
     {
         T f[19];
-        bulk_load<PR>(Pin, ps, 0, G, P, g, i, k, sy, sz, iface, f);
+        bulk_load<PR>(Pin, M, ps, 0, G, g, i, k, sy, sz, iface, f);
         rho = sum19(f);
         T sxm, sym, szm;
         momentum(f, sxm, sym, szm);
         ux = sxm / rho;
         uy = sym / rho;
         uz = szm / rho;
-        eq_poly(ux, uy, uz, poly);
+        PR::poly(ux, uy, uz, poly);
         collide_store<PR>(Pout, ps, g, 0, f, rho, poly, P, T(0));
     }
     // species A and B: the reaction needs both densities before either
@@ -199,31 +247,37 @@ __device__ __forceinline__ void bulk_node(const typename PR::S* __restrict__ Pin
     T ca, cb;
     {
         T a[19];
-        bulk_load<PR>(Pin, ps, 1, G, P, g, i, k, sy, sz, iface, a);
+        bulk_load<PR>(Pin, M, ps, 1, G, g, i, k, sy, sz, iface, a);
         ca = sum19(a);
-        bulk_load<PR>(Pin, ps, 2, G, P, g, i, k, sy, sz, iface, a);
+        bulk_load<PR>(Pin, M, ps, 2, G, g, i, k, sy, sz, iface, a);
         cb = sum19(a);
     }
     const T rt = T(P.rateconst) * ca * cb;
     T cc;
     {
         T a[19];
-        bulk_load<PR>(Pin, ps, 1, G, P, g, i, k, sy, sz, iface, a);
+        bulk_load<PR>(Pin, M, ps, 1, G, g, i, k, sy, sz, iface, a);
         collide_store<PR>(Pout, ps, g, 1, a, ca, poly, P, rt);
-        bulk_load<PR>(Pin, ps, 2, G, P, g, i, k, sy, sz, iface, a);
+        bulk_load<PR>(Pin, M, ps, 2, G, g, i, k, sy, sz, iface, a);
         collide_store<PR>(Pout, ps, g, 2, a, cb, poly, P, rt);
-        bulk_load<PR>(Pin, ps, 3, G, P, g, i, k, sy, sz, iface, a);
+        bulk_load<PR>(Pin, M, ps, 3, G, g, i, k, sy, sz, iface, a);
         cc = sum19(a);
         collide_store<PR>(Pout, ps, g, 3, a, cc, poly, P, rt);
     }
     // densities the junction edges read next step (Tmixer.cpp:8609, :8851)
     if (b == 0 && j == 2 && (i == G.ia || i == G.ib)) {
+        T* Rcur = (T*)X.rcur;
         Rcur[g] = rho;
         Rcur[ps + g] = ca;
         Rcur[2 * ps + g] = cb;
         Rcur[3 * ps + g] = cc;
     }
+    if (PR::kMoments) {
+        X.mcur[g] = make_float4((float)rho, (float)ux, (float)uy, (float)uz);
+        X.mcur[ps + g] = make_float4((float)ca, (float)cb, (float)cc, 0.f);
+    }
     if (write_macro) {
+        double* Mac = X.mac;
         Mac[g] = rho;
         Mac[ps + g] = ux;
         Mac[2 * ps + g] = uy;
@@ -241,6 +295,7 @@ template <class PR>
 struct BCtx {
     using T = typename PR::T;
     const typename PR::S* __restrict__ Pin;
+    const float4* __restrict__ M;  // writers' moments (FP16 form)
     const T* __restrict__ Rprev;
     const T* __restrict__ uin1;
     const T* __restrict__ uin2;
@@ -253,7 +308,7 @@ struct BCtx {
 template <class PR>
 __device__ __forceinline__ typename PR::T own_fn(const BCtx<PR>& c, int fld, int q)
 {
-    return PR::load(c.Pin + (long long)(fld * 19 + q) * c.ps + c.g, PR::shift(fld, q, *c.P));
+    return PR::decode(c.Pin + (long long)(fld * 19 + q) * c.ps + c.g, fld, q, c.M, c.ps, c.g);
 }
 template <class PR>
 __device__ __forceinline__ typename PR::T rprev(const BCtx<PR>& c, int fld, int b, int i, int j, int k)
@@ -274,7 +329,7 @@ __device__ __forceinline__ void pull_node(const BCtx<PR>& c, int fld, int b, int
 #pragma unroll
     for (int q = 0; q < 19; q++) {
         const int s = pull_src(*c.G, b, i, j, k, q);
-        v[q] = s >= 0 ? PR::load(base + (long long)q * c.ps + s, PR::shift(fld, q, *c.P)) : T(0);
+        v[q] = s >= 0 ? PR::decode(base + (long long)q * c.ps + s, fld, q, c.M, c.ps, s) : T(0);
     }
 }
 // the same sum as sum19 without two directions (the closures' "rho - (...)")
@@ -697,23 +752,23 @@ __device__ __forceinline__ void closed_pull(const BCtx<PR>& c, int cls, int fld,
 constexpr int kBoundaryThreads = 128;
 
 template <class PR, bool FACES>
-__device__ __forceinline__ void boundary_node(const typename PR::S* __restrict__ Pin,
-                                              typename PR::S* __restrict__ Pout,
-                                              const typename PR::T* __restrict__ Rprev,
-                                              typename PR::T* __restrict__ Rcur, double* __restrict__ Mac,
-                                              const int* __restrict__ bnode, const unsigned char* __restrict__ bcls,
-                                              int nb, const typename PR::T* __restrict__ uin1,
-                                              const typename PR::T* __restrict__ uin2, const Geom& G, const Phys& P,
-                                              int write_macro, typename PR::T (*stash)[19][kBoundaryThreads])
+__device__ __forceinline__ void boundary_node(const StepPtrs& X, const int* __restrict__ bnode,
+                                              const unsigned char* __restrict__ bcls, int nb, const Geom& G,
+                                              const Phys& P, int write_macro,
+                                              typename PR::T (*stash)[19][kBoundaryThreads])
 {
     using T = typename PR::T;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nb) return;
+    typename PR::S* __restrict__ Pout = (typename PR::S*)X.pout;
+    T* __restrict__ Rcur = (T*)X.rcur;
+    double* __restrict__ Mac = X.mac;
     BCtx<PR> c;
-    c.Pin = Pin;
-    c.Rprev = Rprev;
-    c.uin1 = uin1;
-    c.uin2 = uin2;
+    c.Pin = (const typename PR::S*)X.pin;
+    c.M = X.mprev;
+    c.Rprev = (const T*)X.rprev;
+    c.uin1 = (const T*)X.uin1;
+    c.uin2 = (const T*)X.uin2;
     c.G = &G;
     c.P = &P;
     c.ps = G.ps;
@@ -736,7 +791,7 @@ __device__ __forceinline__ void boundary_node(const typename PR::S* __restrict__
         ux = sxm / rho;
         uy = sym / rho;
         uz = szm / rho;
-        eq_poly(ux, uy, uz, poly);
+        PR::poly(ux, uy, uz, poly);
         collide_store<PR>(Pout, ps, c.g, 0, f, rho, poly, P, T(0));
     }
     T ca, cb, cc;
@@ -769,6 +824,10 @@ __device__ __forceinline__ void boundary_node(const typename PR::S* __restrict__
     Rcur[ps + c.g] = ca;
     Rcur[2 * ps + c.g] = cb;
     Rcur[3 * ps + c.g] = cc;
+    if (PR::kMoments) {
+        X.mcur[c.g] = make_float4((float)rho, (float)ux, (float)uy, (float)uz);
+        X.mcur[ps + c.g] = make_float4((float)ca, (float)cb, (float)cc, 0.f);
+    }
     if (write_macro) {
         Mac[c.g] = rho;
         Mac[ps + c.g] = ux;
@@ -782,35 +841,27 @@ __device__ __forceinline__ void boundary_node(const typename PR::S* __restrict__
 
 // Kernel definitions for one precision policy; NAME is the kernel-name suffix.
 #define TMX_DEFINE_STEP_KERNELS(PR, NAME)                                                                         \
-    __global__ void k_init_##NAME(void* Pout, void* R, double* Mac, Geom G, Phys P, double rho0)                \
+    __global__ void k_init_##NAME(StepPtrs X, Geom G, Phys P, double rho0)                                      \
     {                                                                                                           \
         for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < G.nnodes; g += gridDim.x * blockDim.x)          \
-            init_node<PR>((PR::S*)Pout, (PR::T*)R, Mac, G, P, rho0, g);                                         \
+            init_node<PR>(X, G, P, rho0, g);                                                                    \
     }                                                                                                           \
-    __global__ void __launch_bounds__(256, 2)                                                                   \
-        k_bulk_##NAME(const void* Pin, void* Pout, void* Rcur, double* Mac, Geom G, Phys P, int write_macro)    \
+    __global__ void __launch_bounds__(256, 2) k_bulk_##NAME(StepPtrs X, Geom G, Phys P, int write_macro)        \
     {                                                                                                           \
         for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < G.nnodes; g += gridDim.x * blockDim.x)          \
-            bulk_node<PR>((const PR::S*)Pin, (PR::S*)Pout, (PR::T*)Rcur, Mac, G, P, write_macro, g);            \
+            bulk_node<PR>(X, G, P, write_macro, g);                                                             \
     }                                                                                                           \
-    __global__ void __launch_bounds__(kBoundaryThreads)                                                        \
-        k_bfaces_##NAME(const void* Pin, void* Pout, const void* Rprev, void* Rcur, double* Mac,                \
-                        const int* bnode, const unsigned char* bcls, int nb, const void* uin1, const void* uin2, \
-                        Geom G, Phys P, int write_macro)                                                        \
+    __global__ void __launch_bounds__(kBoundaryThreads) k_bfaces_##NAME(                                       \
+        StepPtrs X, const int* bnode, const unsigned char* bcls, int nb, Geom G, Phys P, int write_macro)       \
     {                                                                                                           \
         __shared__ PR::T stash[2][19][kBoundaryThreads];                                                        \
-        boundary_node<PR, true>((const PR::S*)Pin, (PR::S*)Pout, (const PR::T*)Rprev, (PR::T*)Rcur, Mac, bnode, \
-                                bcls, nb, (const PR::T*)uin1, (const PR::T*)uin2, G, P, write_macro, stash);    \
+        boundary_node<PR, true>(X, bnode, bcls, nb, G, P, write_macro, stash);                                  \
     }                                                                                                           \
-    __global__ void __launch_bounds__(kBoundaryThreads)                                                        \
-        k_bedges_##NAME(const void* Pin, void* Pout, const void* Rprev, void* Rcur, double* Mac,                \
-                        const int* bnode, const unsigned char* bcls, int nb, const void* uin1, const void* uin2, \
-                        Geom G, Phys P, int write_macro)                                                        \
+    __global__ void __launch_bounds__(kBoundaryThreads) k_bedges_##NAME(                                       \
+        StepPtrs X, const int* bnode, const unsigned char* bcls, int nb, Geom G, Phys P, int write_macro)       \
     {                                                                                                           \
         __shared__ PR::T stash[2][19][kBoundaryThreads];                                                        \
-        boundary_node<PR, false>((const PR::S*)Pin, (PR::S*)Pout, (const PR::T*)Rprev, (PR::T*)Rcur, Mac,       \
-                                 bnode, bcls, nb, (const PR::T*)uin1, (const PR::T*)uin2, G, P, write_macro,    \
-                                 stash);                                                                        \
+        boundary_node<PR, false>(X, bnode, bcls, nb, G, P, write_macro, stash);                                 \
     }
 
 }  // namespace tmx

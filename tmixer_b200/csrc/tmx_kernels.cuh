@@ -7,18 +7,30 @@
 
 namespace tmx {
 
+// Buffers of one step (populations in/out, boundary densities previous/this
+// step, macroscopic fields, FP16-form moments previous/this step, inlet
+// profiles); the kernels cast to the form's types.
+struct StepPtrs {
+    const void* pin;
+    void* pout;
+    const void* rprev;
+    void* rcur;
+    double* mac;
+    const float4* mprev;
+    float4* mcur;
+    const void* uin1;
+    const void* uin2;
+};
+
 constexpr int kBoundaryThreadsHost = 128;  // block size of the boundary kernels
 
 #define TMX_DECLARE_STEP_KERNELS(NAME)                                                                          \
-    __global__ void k_init_##NAME(void* Pout, void* R, double* Mac, Geom G, Phys P, double rho0);              \
-    __global__ void k_bulk_##NAME(const void* Pin, void* Pout, void* Rcur, double* Mac, Geom G, Phys P,         \
-                                  int write_macro);                                                             \
-    __global__ void k_bfaces_##NAME(const void* Pin, void* Pout, const void* Rprev, void* Rcur, double* Mac,    \
-                                    const int* bnode, const unsigned char* bcls, int nb, const void* uin1,      \
-                                    const void* uin2, Geom G, Phys P, int write_macro);                         \
-    __global__ void k_bedges_##NAME(const void* Pin, void* Pout, const void* Rprev, void* Rcur, double* Mac,    \
-                                    const int* bnode, const unsigned char* bcls, int nb, const void* uin1,      \
-                                    const void* uin2, Geom G, Phys P, int write_macro);
+    __global__ void k_init_##NAME(StepPtrs X, Geom G, Phys P, double rho0);                                     \
+    __global__ void k_bulk_##NAME(StepPtrs X, Geom G, Phys P, int write_macro);                                 \
+    __global__ void k_bfaces_##NAME(StepPtrs X, const int* bnode, const unsigned char* bcls, int nb, Geom G,    \
+                                    Phys P, int write_macro);                                                   \
+    __global__ void k_bedges_##NAME(StepPtrs X, const int* bnode, const unsigned char* bcls, int nb, Geom G,    \
+                                    Phys P, int write_macro);
 
 TMX_DECLARE_STEP_KERNELS(f64)
 TMX_DECLARE_STEP_KERNELS(f32)
