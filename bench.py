@@ -3,8 +3,10 @@
 
 Workload (N=1): the single-mixer configuration of the benchmark set, a T-mixer
 of width W=32 (inlet 256x32x32, mixing 64x128x32: 524,288 fluid nodes), flow
-tau 0.56, species tau 0.6, k = 1e-3, inlet profile maximum 0.05, outlet and
-initial density 1, in the plain FP64 form (bit-exact with the reference).
+tau 0.6 (see WORKLOAD), species tau 0.6, k = 1e-3, inlet profile maximum 0.05,
+outlet and initial density 1, by default in the plain FP64 form (bit-exact with
+the reference); --form fp32 / fp16 selects a reduced-precision form, and the
+line always carries all three forms' throughput under "forms".
 A "step" is one full lattice-Boltzmann time step of the mixer (flow + 3
 species, all nodes); MLUPS counts node updates of all four fields.
 
@@ -15,9 +17,10 @@ species, all nodes); MLUPS counts node updates of all four fields.
   e2e        the whole configured solve (create, init with the host inlet
              profile, 20,000 steps with the outlet mixing index read back every
              100 steps, all fields copied to host) through the public API.
-  roofline   the bulk (interior) kernel: 1216 algorithmic bytes per node
-             update (76 FP64 populations read and written) over its average
-             launch time, against the measured HBM copy bandwidth.
+  roofline   the bulk (interior) kernel: algorithmic bytes per node update
+             (76 populations read and written: 1216 B FP64, 608 B FP32; the
+             FP16 form 304 B + 64 B of moments) over its average launch time,
+             against the measured HBM copy bandwidth.
   cpu_baseline  the reference's own OpenMP build (oracle/_ref) on this host's
              cores, on a bounded number of steps of the same workload.
 
@@ -42,8 +45,18 @@ sys.path.insert(0, ROOT)
 
 METRIC = "MLUPS & %HBM roofline, served FP16-storage vs plain FP64; p50/p99 solve latency"
 UNIT = "MLUPS"
-WORKLOAD = dict(W=32, u_max=0.05, tau_f=0.56, tau_c=0.6, k=1e-3, rho=1.0, steps=20000)
+# The single-mixer configuration (W=32, u_max 0.05, tau_c 0.6, k 1e-3, rho 1,
+# 20000 steps) with the flow relaxation time of the reference case, 0.6: at
+# the configuration's 0.56 the reference's own boundary closures diverge (the
+# reference-exact oracle and the FP64 GPU form both turn non-finite after about
+# 1000 steps, even at u_max 0.02), and a step costs the same at either value.
+WORKLOAD = dict(W=32, u_max=0.05, tau_f=0.6, tau_c=0.6, k=1e-3, rho=1.0, steps=20000)
+CONFIG_TAU_F = 0.56
 BYTES_PER_LUP_FP64 = 4 * 19 * 8 * 2
+# algorithmic bytes per lattice update of each form: populations read + written
+# (76 values), plus for the FP16 form the writer's FP32 moments (2 x float4)
+# written once and read once
+FORM_BYTES = {"fp64": 1216, "fp32": 608, "fp16": 304 + 64}
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -56,11 +69,12 @@ def measured_peaks() -> dict:
     return dict(hbm_gbs=FALLBACK_HBM_GBS, source="fallback")
 
 
-def workload_spec():
+def workload_spec(form: str = "fp64"):
     import tmixer_b200 as T
 
     w = WORKLOAD
-    return T.w_layout(w["W"], w["u_max"], w["tau_f"], w["tau_c"], w["k"], w["rho"], steps=w["steps"])
+    return T.w_layout(w["W"], w["u_max"], w["tau_f"], w["tau_c"], w["k"], w["rho"], steps=w["steps"],
+                      precision=T.PRECISIONS[form])
 
 
 def workload_ref_params(spec) -> dict:
@@ -75,7 +89,9 @@ def config_dict(spec, form: str, n_gpus: int) -> dict:
                         % (WORKLOAD["W"], spec.inx, spec.iny, spec.nz, spec.mnx, spec.mny, spec.nz, spec.nodes(),
                            form),
             "form": form, "fluid_nodes": spec.nodes(), "bbox_nodes": spec.inx * (spec.iny + spec.mny) * spec.nz,
-            "tau_f": spec.tau, "tau_c": spec.tau_a, "k": spec.rateconst, "u_max": WORKLOAD["u_max"],
+            "tau_f": spec.tau, "tau_f_note": "configuration says %.2f; the reference's closures diverge there"
+                                             % CONFIG_TAU_F,
+            "tau_c": spec.tau_a, "k": spec.rateconst, "u_max": WORKLOAD["u_max"],
             "solve_steps": WORKLOAD["steps"], "parallelism": "replicas x%d" % n_gpus,
             "l2": "state (2 x 319 MB) larger than L2, no flush"}
 
@@ -209,9 +225,9 @@ def reference_cpu_run(spec, budget_s: float, max_steps: int | None = None) -> di
             "seconds": secs, "steps": n}
 
 
-def profile_traffic() -> dict | None:
+def profile_traffic(form: str = "fp64") -> dict | None:
     """DRAM bytes per launch of the bulk kernel from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "k_bulk_fp64_w32.json")
+    p = os.path.join(ROOT, "profiles", "k_bulk_%s_w32.json" % form)
     if not os.path.exists(p):
         return None
     with open(p) as fh:
@@ -227,46 +243,60 @@ def run_ours(args, dist: Dist) -> dict | None:
     torch.cuda.set_device(dist.local_rank)
     dist.init("nccl")
     dev = torch.device("cuda", dist.local_rank)
-    spec = workload_spec()
+    spec = workload_spec(args.form)
     nodes = spec.nodes()
     peaks = measured_peaks()
 
-    s = T.Solver(spec, device=dist.local_rank).init()
-    s.step(args.warmup)
-    s.sync()
-    counts = s.counts()
+    def measure(form: str, steps: int, warmup: int, clocks=None):
+        """K steps of one form (events on the solver's stream, max over
+        ranks), then per-launch kernel times for the roofline."""
+        sp = workload_spec(form)
+        s = T.Solver(sp, device=dist.local_rank).init()
+        s.step(warmup)
+        s.sync()
+        counts = s.counts()
+        torch.cuda.synchronize()
+        dist.barrier()
+        if clocks:
+            clocks.start()
+        ms = s.time_steps(steps)
+        torch.cuda.synchronize()
+        dist.barrier()
+        clk = clocks.stop() if clocks else None
+        ms_max = dist.max(ms, dev)
+        kr = min(steps, 400)
+        tb, tbd, _ = s.step_timed(kr)
+        s.close()
+        bulk_ms, bnd_ms = tb / kr, tbd / kr
+        bpl = FORM_BYTES[form]
+        bulk_bytes = counts["interior"] * bpl
+        achieved = bulk_bytes / (bulk_ms * 1e-3) / 1e9
+        return dict(counts=counts, ms_max=ms_max, clk=clk, bulk_ms=bulk_ms, bnd_ms=bnd_ms, bulk_bytes=bulk_bytes,
+                    achieved=achieved, mlups=dist.world * nodes * steps / (ms_max * 1e-3) / 1e6,
+                    step_gbs=nodes * bpl / (ms_max / steps * 1e-3) / 1e9)
 
-    # --- value: K steps, events on the solver's stream, max over ranks ----
-    clocks = ClockSampler(dist.local_rank)
-    torch.cuda.synchronize()
-    dist.barrier()
-    clocks.start()
-    ms = s.time_steps(args.steps)
-    torch.cuda.synchronize()
-    dist.barrier()
-    clk = clocks.stop()
-    ms_max = dist.max(ms, dev)
-    value = dist.world * nodes * args.steps / (ms_max * 1e-3) / 1e6
-
-    # --- roofline of the dominant kernel: per-launch events --------------
-    kr = min(args.steps, 400)
-    tb, tbd, tt = s.step_timed(kr)
-    bulk_ms = tb / kr
-    bnd_ms = tbd / kr
-    bulk_bytes = counts["interior"] * BYTES_PER_LUP_FP64
-    achieved = bulk_bytes / (bulk_ms * 1e-3) / 1e9
-    prof = profile_traffic()
-    traffic = None
-    if prof and prof.get("nodes") == nodes:
-        traffic = prof.get("dram_bytes_per_launch")
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
-                "kernel": "k_bulk (interior nodes, %d per launch)" % counts["interior"],
+    # --- value: K steps of the main form -----------------------------------
+    main = measure(args.form, args.steps, args.warmup, ClockSampler(dist.local_rank))
+    counts, ms_max, clk, value = main["counts"], main["ms_max"], main["clk"], main["mlups"]
+    prof = profile_traffic(args.form)
+    traffic = prof.get("dram_bytes_per_launch") if prof and prof.get("nodes") == nodes else None
+    roofline = {"bound": "hbm", "achieved": main["achieved"], "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": main["achieved"] / peaks["hbm_gbs"], "traffic": traffic,
+                "kernel": "k_bulk_%s (interior nodes, %d per launch)" % (args.form, counts["interior"]),
                 "peak_source": peaks["source"],
-                "algorithmic_bytes_per_launch": bulk_bytes,
-                "boundary_kernel_ms": bnd_ms, "bulk_kernel_ms": bulk_ms,
-                "step_effective_gbs": nodes * BYTES_PER_LUP_FP64 / (ms_max / args.steps * 1e-3) / 1e9}
-    s.close()
+                "algorithmic_bytes_per_lup": FORM_BYTES[args.form],
+                "algorithmic_bytes_per_launch": main["bulk_bytes"],
+                "boundary_kernels_ms": main["bnd_ms"], "bulk_kernel_ms": main["bulk_ms"],
+                "step_effective_gbs": main["step_gbs"]}
+    # --- the other forms, for comparison (same workload) --------------------
+    forms = {}
+    if not args.no_forms:
+        for form in ("fp64", "fp32", "fp16"):
+            m = main if form == args.form else measure(form, min(args.steps, 1000), args.warmup)
+            forms[form] = {"mlups": m["mlups"], "ms_per_step": m["ms_max"] / (args.steps if form == args.form
+                                                                               else min(args.steps, 1000)),
+                           "bulk_gbs": m["achieved"], "bulk_frac": m["achieved"] / peaks["hbm_gbs"],
+                           "bytes_per_lup": FORM_BYTES[form]}
 
     # --- e2e: the configured solve through the public API ---------------
     e2e_steps = args.e2e_steps
@@ -299,12 +329,15 @@ def run_ours(args, dist: Dist) -> dict | None:
     dist.close()
     if dist.rank != 0:
         return None
+    form_text = {"fp64": "plain FP64 (bit-exact with the reference)", "fp32": "FP32 storage and arithmetic",
+                 "fp16": "FP32 arithmetic, FP16 storage of the non-equilibrium populations + FP32 moments"}
     return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": config_dict(spec, "plain FP64 (bit-exact with the reference)", dist.world),
+            "scaling": "weak", "vs_baseline": None, "dtype": {"fp64": "f64", "fp32": "f32", "fp16": "f32/f16"}[args.form],
+            "data": "synthetic",
+            "config": config_dict(spec, form_text[args.form], dist.world),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
-            "gpu_launches": 2 * args.steps}
+            "gpu_launches": 3 * args.steps, "forms": forms}
 
 
 def run_reference(args, dist: Dist) -> dict | None:
@@ -333,6 +366,9 @@ def main(argv=None) -> int:
     ap.add_argument("--e2e-steps", type=int, default=WORKLOAD["steps"])
     ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of reference CPU steps")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--form", choices=["fp64", "fp32", "fp16"], default="fp64",
+                    help="form of the main line (fp64: the plain form, bit-exact with the reference)")
+    ap.add_argument("--no-forms", action="store_true", help="skip the comparison of the three forms")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

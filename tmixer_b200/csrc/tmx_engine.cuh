@@ -58,6 +58,7 @@ struct F64 {
     using T = double;
     using S = double;
     static constexpr bool kMoments = false;
+    static constexpr bool kOnePass = false;  // 76 FP64 values exceed the register budget
     __device__ static void poly(T ux, T uy, T uz, T (&p)[19]) { eq_poly(ux, uy, uz, p); }
     __device__ static bool tiny(T r) { return tiny_density(r); }
     __device__ static T feq(T r, T polyq, int q, bool tiny)
@@ -67,6 +68,7 @@ struct F64 {
     }
     __device__ static T decode(const S* p, int, int, const float4*, long long, int) { return __ldg(p); }
     __device__ static void encode(S* p, T v, T) { *p = v; }
+    __device__ static T raw(const S* p) { return __ldg(p); }
 };
 
 // FP32 arithmetic and storage.
@@ -74,11 +76,13 @@ struct F32 {
     using T = float;
     using S = float;
     static constexpr bool kMoments = false;
+    static constexpr bool kOnePass = true;
     __device__ static void poly(T ux, T uy, T uz, T (&p)[19]) { eq_poly(ux, uy, uz, p); }
     __device__ static bool tiny(T) { return false; }
     __device__ static T feq(T r, T polyq, int q, bool) { return r * polyq * (float)wq(q); }
     __device__ static T decode(const S* p, int, int, const float4*, long long, int) { return __ldg(p); }
     __device__ static void encode(S* p, T v, T) { *p = v; }
+    __device__ static T raw(const S* p) { return __ldg(p); }
 };
 
 // FP32 arithmetic; populations stored in FP16 as their non-equilibrium part
@@ -90,6 +94,7 @@ struct F16 {
     using T = float;
     using S = __half;
     static constexpr bool kMoments = true;
+    static constexpr bool kOnePass = true;
     __device__ static void poly(T ux, T uy, T uz, T (&p)[19])
     {
 #pragma unroll
@@ -108,6 +113,7 @@ struct F16 {
         return __half2float(__ldg(p)) + feq(r, poly_q_rn(q, mf.y, mf.z, mf.w), q, false);
     }
     __device__ static void encode(S* p, T v, T feq) { *p = __float2half_rn(v - feq); }
+    __device__ static T raw(const S* p) { return __half2float(__ldg(p)); }
 };
 
 
@@ -265,6 +271,78 @@ __device__ __forceinline__ void bulk_node(const StepPtrs& X, const Geom& G, cons
         collide_store<PR>(Pout, ps, g, 3, a, cc, poly, P, rt);
     }
     // densities the junction edges read next step (Tmixer.cpp:8609, :8851)
+    if (b == 0 && j == 2 && (i == G.ia || i == G.ib)) {
+        T* Rcur = (T*)X.rcur;
+        Rcur[g] = rho;
+        Rcur[ps + g] = ca;
+        Rcur[2 * ps + g] = cb;
+        Rcur[3 * ps + g] = cc;
+    }
+    if (PR::kMoments) {
+        X.mcur[g] = make_float4((float)rho, (float)ux, (float)uy, (float)uz);
+        X.mcur[ps + g] = make_float4((float)ca, (float)cb, (float)cc, 0.f);
+    }
+    if (write_macro) {
+        double* Mac = X.mac;
+        Mac[g] = rho;
+        Mac[ps + g] = ux;
+        Mac[2 * ps + g] = uy;
+        Mac[3 * ps + g] = uz;
+        Mac[4 * ps + g] = ca;
+        Mac[5 * ps + g] = cb;
+        Mac[6 * ps + g] = cc;
+    }
+}
+
+// One interior node for the reduced-precision forms (FP32 arithmetic): every
+// source index and (FP16 form) every writer's moments are fetched once per
+// direction and all 76 populations decoded in one pass, which the FP32
+// register budget affords (the FP64 form above loads field by field).
+template <class PR>
+__device__ __forceinline__ void bulk_node_lp(const StepPtrs& X, const Geom& G, const Phys& P, int write_macro, int g)
+{
+    using T = typename PR::T;
+    const typename PR::S* __restrict__ Pin = (const typename PR::S*)X.pin;
+    typename PR::S* __restrict__ Pout = (typename PR::S*)X.pout;
+    const float4* __restrict__ M = X.mprev;
+    const long long ps = G.ps;
+    int b, i, j, k;
+    decode(G, g, b, i, j, k);
+    if (is_boundary(G, b, i, j, k)) return;
+    const int sy = G.nx[b], sz = G.nx[b] * G.ny[b];
+    const int iface = (b == 0 && j == 1) ? 1 : ((b == 1 && j == G.mny) ? 2 : 0);
+
+    T f[19], a[19], bb[19], c[19];
+#pragma unroll
+    for (int q = 0; q < 19; q++) {
+        const int s = bulk_src(G, g, i, k, sy, sz, iface, q);
+        const typename PR::S* p = Pin + (long long)q * ps + s;
+        T e0 = T(0), e1 = T(0), e2 = T(0), e3 = T(0);
+        if (PR::kMoments) {
+            const float4 mf = __ldg(M + s), ms = __ldg(M + ps + s);
+            const float pq = poly_q_rn(q, mf.y, mf.z, mf.w);
+            e0 = PR::feq(mf.x, pq, q, false);
+            e1 = PR::feq(ms.x, pq, q, false);
+            e2 = PR::feq(ms.y, pq, q, false);
+            e3 = PR::feq(ms.z, pq, q, false);
+        }
+        f[q] = PR::raw(p) + e0;
+        a[q] = PR::raw(p + 19 * ps) + e1;
+        bb[q] = PR::raw(p + 38 * ps) + e2;
+        c[q] = PR::raw(p + 57 * ps) + e3;
+    }
+    const T rho = sum19(f);
+    T sxm, sym, szm;
+    momentum(f, sxm, sym, szm);
+    const T ux = sxm / rho, uy = sym / rho, uz = szm / rho;
+    T poly[19];
+    PR::poly(ux, uy, uz, poly);
+    const T ca = sum19(a), cb = sum19(bb), cc = sum19(c);
+    const T rt = T(P.rateconst) * ca * cb;
+    collide_store<PR>(Pout, ps, g, 0, f, rho, poly, P, T(0));
+    collide_store<PR>(Pout, ps, g, 1, a, ca, poly, P, rt);
+    collide_store<PR>(Pout, ps, g, 2, bb, cb, poly, P, rt);
+    collide_store<PR>(Pout, ps, g, 3, c, cc, poly, P, rt);
     if (b == 0 && j == 2 && (i == G.ia || i == G.ib)) {
         T* Rcur = (T*)X.rcur;
         Rcur[g] = rho;
@@ -849,7 +927,10 @@ __device__ __forceinline__ void boundary_node(const StepPtrs& X, const int* __re
     __global__ void __launch_bounds__(256, 2) k_bulk_##NAME(StepPtrs X, Geom G, Phys P, int write_macro)        \
     {                                                                                                           \
         for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < G.nnodes; g += gridDim.x * blockDim.x)          \
-            bulk_node<PR>(X, G, P, write_macro, g);                                                             \
+            if (PR::kOnePass)                                                                                   \
+                bulk_node_lp<PR>(X, G, P, write_macro, g);                                                      \
+            else                                                                                                \
+                bulk_node<PR>(X, G, P, write_macro, g);                                                         \
     }                                                                                                           \
     __global__ void __launch_bounds__(kBoundaryThreads) k_bfaces_##NAME(                                       \
         StepPtrs X, const int* bnode, const unsigned char* bcls, int nb, Geom G, Phys P, int write_macro)       \
