@@ -142,6 +142,23 @@ int tmx_populations(tmx_handle *h, int box, int fld, double *host_out);
  * (Tmixer.cpp:10161-10409), with its running maxima starting at 0. */
 int tmx_mixing(tmx_handle *h, double *rows_out, double *outlet_im);
 
+/* tmx_mixing without any allocation, host or device, in the call: the same
+ * rows, bit for bit, from a fixed 512 KiB scratch array in the library's
+ * static device memory, finished on the device and copied straight into
+ * rows_out.  No counterpart in the reference.  For callers that must not
+ * allocate while they poll the mixing quality, such as a monitor thread
+ * that may not take the heap lock or a host that accounts for every byte of
+ * device memory itself.
+ *   - At most 4096 rows (mny + iny <= 4096); larger cases get TMX_E_INVALID
+ *     (use tmx_mixing).
+ *   - The first call on each device resolves the scratch address there
+ *     (cudaGetSymbolAddress); make it before capturing any stream on that
+ *     device.
+ *   - The scratch is shared by every handle of the process on that device:
+ *     calls that overlap in time on one device race and must be serialised
+ *     by the caller. */
+int tmx_mixing_static(tmx_handle *h, double *rows_out, double *outlet_im);
+
 /* FP64 totals over both boxes after the last step: out[0] = sum rho,
  * out[1..3] = sum cA, cB, cC, out[4] = sum (cA + cB + cC), out[5] = outlet
  * flux sum(rho*uy) over mixing row 1, out[6] = number of non-finite values in

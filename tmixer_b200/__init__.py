@@ -80,6 +80,7 @@ def lib() -> ctypes.CDLL:
     L.tmx_fields.argtypes = [vp, ip, ip, vp]
     L.tmx_populations.argtypes = [vp, ip, ip, vp]
     L.tmx_mixing.argtypes = [vp, vp, vp]
+    L.tmx_mixing_static.argtypes = [vp, vp, vp]
     L.tmx_sums.argtypes = [vp, vp]
     L.tmx_inlet_profile.argtypes = [vp, vp, vp]
     L.tmx_step_timed.argtypes = [vp, ip, P(dp), P(dp), P(dp)]
@@ -251,6 +252,14 @@ class Solver:
         rows = np.empty((self.spec.mny + self.spec.iny, 7), dtype=np.float64)
         im = np.empty(3, dtype=np.float64)
         _check(lib().tmx_mixing(self._h, rows.ctypes.data, im.ctypes.data))
+        return rows, im
+
+    def mixing_static(self):
+        """tmx_mixing_static: the rows of mixing() with no allocation inside
+        the library call (fixed static device scratch, at most 4096 rows)."""
+        rows = np.empty((self.spec.mny + self.spec.iny, 7), dtype=np.float64)
+        im = np.empty(3, dtype=np.float64)
+        _check(lib().tmx_mixing_static(self._h, rows.ctypes.data, im.ctypes.data))
         return rows, im
 
     def sums(self) -> np.ndarray:

@@ -11,6 +11,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -741,6 +742,46 @@ int tmx_mixing(tmx_handle* h, double* rows_out, double* outlet_im)
             }
         }
     }
+    if (outlet_im)
+        for (int q = 0; q < 3; q++) outlet_im[q] = rows_out[4 + q];
+    return TMX_OK;
+}
+
+// Scratch address of tmx_mixing_static per device, resolved by the first
+// call on that device (cudaGetSymbolAddress with the device current).
+namespace {
+constexpr int kMixStaticDevices = 64;
+std::once_flag g_mix_once[kMixStaticDevices];
+double* g_mix_ptr[kMixStaticDevices];
+cudaError_t g_mix_err[kMixStaticDevices];
+}  // namespace
+
+int tmx_mixing_static(tmx_handle* h, double* rows_out, double* outlet_im)
+{
+    if (!h || !rows_out) return fail(TMX_E_INVALID, "null argument");
+    if (!h->inited) return fail(TMX_E_STATE, "tmx_mixing_static before tmx_init");
+    const Geom& G = h->G;
+    const int nrow = G.mny + G.iny;
+    if (nrow > tmx::kMixStaticRows)
+        return fail(TMX_E_INVALID,
+                    "tmx_mixing_static: mny + iny = %d rows exceeds its fixed scratch of %d rows (use tmx_mixing)",
+                    nrow, tmx::kMixStaticRows);
+    const int d = h->device;
+    if (d < 0 || d >= kMixStaticDevices)
+        return fail(TMX_E_INVALID, "tmx_mixing_static: device %d is beyond its table of %d devices", d,
+                    kMixStaticDevices);
+    TMX_CK(cudaSetDevice(d));
+    std::call_once(g_mix_once[d], [d] { g_mix_err[d] = tmx::mixing_static_scratch(&g_mix_ptr[d]); });
+    if (g_mix_err[d] != cudaSuccess)
+        return fail(TMX_E_CUDA, "tmx_mixing_static: cudaGetSymbolAddress on device %d: %s", d,
+                    cudaGetErrorString(g_mix_err[d]));
+    double* stats = g_mix_ptr[d];
+    double* rows = stats + (size_t)tmx::kMixStaticRows * 9;
+    tmx::k_mixing_rows<<<nrow, 32, 0, h->stream>>>(h->mac, G, stats);
+    tmx::k_mixing_finish<<<1, 96, 0, h->stream>>>(stats, G, rows);
+    TMX_CK(cudaGetLastError());
+    TMX_CK(cudaMemcpyAsync(rows_out, rows, (size_t)nrow * 7 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    TMX_CK(cudaStreamSynchronize(h->stream));
     if (outlet_im)
         for (int q = 0; q < 3; q++) outlet_im[q] = rows_out[4 + q];
     return TMX_OK;

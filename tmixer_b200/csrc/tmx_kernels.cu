@@ -52,6 +52,53 @@ __global__ void k_mixing_rows(const double* __restrict__ Mac, Geom G, double* __
 }
 
 // ---------------------------------------------------------------------------
+// Fixed device scratch of tmx_mixing_static (no allocation in that call).
+// Every word the call reads is written earlier in the same call, so nothing
+// in it has to start at zero.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) double g_mix_scratch[kMixStaticRows * (9 + 7)];
+
+cudaError_t mixing_static_scratch(double** ptr) { return cudaGetSymbolAddress((void**)ptr, g_mix_scratch); }
+
+// Finish the rows of write_MixingQuality() (Tmixer.cpp:10161-10409) on the
+// device, with the same arithmetic as the host finish of tmx_mixing: running
+// maxima over the rows in the reference's order starting at 0, then
+// I_s = 1 - sqrt(var / (avg * (max - avg))).  One warp per species; lane l
+// takes a contiguous chunk of rows, and a shuffle scan of the chunk maxima
+// gives each chunk its running maximum on entry.  The update "if (m < v)
+// m = v" from 0 keeps m = max(+0, non-NaN values), whatever the grouping, so
+// the chunked scan equals the sequential one bit for bit.
+__global__ void k_mixing_finish(const double* __restrict__ stats, Geom G, double* __restrict__ rows)
+{
+    const int q = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (q >= 3) return;
+    const int nrow = G.mny + G.iny;
+    const int chunk = (nrow + 31) / 32;
+    const int r0 = min(lane * chunk, nrow), r1 = min(r0 + chunk, nrow);
+    double m = 0.0;
+    for (int r = r0; r < r1; r++) {
+        const double v = stats[r * 9 + 6 + q];
+        if (m < v) m = v;
+    }
+    for (int o = 1; o < 32; o <<= 1) {
+        const double y = __shfl_up_sync(0xffffffffu, m, o);
+        if (lane >= o && m < y) m = y;
+    }
+    double mx = __shfl_up_sync(0xffffffffu, m, 1);
+    if (lane == 0) mx = 0.0;
+    for (int r = r0; r < r1; r++) {
+        const double* s = stats + r * 9;
+        double* o = rows + r * 7;
+        const bool mixing_row = r < G.mny;
+        if (q == 0) o[0] = mixing_row ? r + 1 : (r - G.mny + 1) + G.mny;
+        if (mx < s[6 + q]) mx = s[6 + q];
+        o[1 + q] = s[q];
+        const bool ok = mixing_row ? (s[0] > 0 && s[1] > 0 && s[2] > 0) : (s[0] > 0);
+        o[4 + q] = ok ? 1.0 - sqrt(s[3 + q] / (s[q] * (mx - s[q]))) : 0.0;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // FP64 totals: warp-shuffle block reduction, one partial per block
 // ---------------------------------------------------------------------------
 __global__ void k_sums(const double* __restrict__ Mac, Geom G, double* __restrict__ partial)

@@ -39,4 +39,11 @@ TMX_DECLARE_STEP_KERNELS(f16)
 __global__ void k_mixing_rows(const double* __restrict__ Mac, Geom G, double* __restrict__ stats);
 __global__ void k_sums(const double* __restrict__ Mac, Geom G, double* __restrict__ partial);
 
+// Fixed scratch of tmx_mixing_static: kMixStaticRows rows of 9 statistics
+// followed by kMixStaticRows finished rows of 7 numbers (512 KiB per device).
+constexpr int kMixStaticRows = 4096;
+__global__ void k_mixing_finish(const double* __restrict__ stats, Geom G, double* __restrict__ rows);
+// Device address of that scratch on the current device.
+cudaError_t mixing_static_scratch(double** ptr);
+
 }  // namespace tmx
