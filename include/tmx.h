@@ -37,7 +37,7 @@ extern "C" {
 /* arithmetic of the state and of the step */
 #define TMX_FP64 0 /* plain form: FP64 storage and arithmetic, bit-exact with the reference */
 #define TMX_FP32 1 /* FP32 storage and arithmetic */
-#define TMX_FP16 2 /* FP32 arithmetic, populations stored in FP16 as f_q - w_q*rho0 (flow) and g_q (species) */
+#define TMX_FP16 2 /* FP32 arithmetic; populations stored in FP16 as their non-equilibrium part, next to FP32 moments */
 
 /* field ids of tmx_fields */
 #define TMX_RHO 0

@@ -30,7 +30,7 @@ LIB_PATH = os.path.join(_PKG, "libtmx.so")
 FIELDS = ("rho", "ux", "uy", "uz", "cA", "cB", "cC")
 TMX_FP64 = 0  # plain form, bit-exact with the reference
 TMX_FP32 = 1  # FP32 storage and arithmetic
-TMX_FP16 = 2  # FP32 arithmetic, populations stored in FP16 (flow shifted by w_q*rho0)
+TMX_FP16 = 2  # FP32 arithmetic, populations stored in FP16 as f_q - feq_q of the writing node
 PRECISIONS = {"fp64": TMX_FP64, "fp32": TMX_FP32, "fp16": TMX_FP16}
 ABI_VERSION = 1
 

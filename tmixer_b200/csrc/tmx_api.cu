@@ -676,7 +676,7 @@ int tmx_populations(tmx_handle* h, int box, int fld, double* host_out)
     // reduced precision: widen on the host; the FP16 form adds back feq of
     // the writing node's moments exactly as the kernels do (tmx_engine.cuh)
     std::vector<double> wide(n);
-    std::vector<unsigned char> raw(n * h->sbytes);
+    std::vector<unsigned char> raw(4 * n * h->sbytes);
     std::vector<float> mf(4 * n), ms(4 * n);
     if (h->K->moments) {
         const float4* m = h->mom[h->cur];
@@ -684,17 +684,19 @@ int tmx_populations(tmx_handle* h, int box, int fld, double* host_out)
         TMX_CK(cudaMemcpy(ms.data(), m + G.ps + G.base[box], n * sizeof(float4), cudaMemcpyDeviceToHost));
     }
     for (int q = 0; q < 19; q++) {
+        // interleaved layout: the four fields of (q, node) side by side
         const unsigned char* src =
-            (const unsigned char*)h->pop[h->cur] + ((size_t)(fld * 19 + q) * G.ps + G.base[box]) * h->sbytes;
+            (const unsigned char*)h->pop[h->cur] + ((size_t)q * G.ps + G.base[box]) * 4 * h->sbytes;
         TMX_CK(cudaMemcpy(raw.data(), src, raw.size(), cudaMemcpyDeviceToHost));
         const float w = (float)(q == 0 ? 1.0 / 3.0 : (q <= 6 ? 1.0 / 18.0 : 1.0 / 36.0));
         for (size_t t = 0; t < n; t++) {
             float v;
+            const size_t e = (t * 4 + fld) * h->sbytes;
             if (h->sbytes == 4) {
-                std::memcpy(&v, &raw[t * 4], 4);
+                std::memcpy(&v, &raw[e], 4);
             } else {
                 unsigned short hb;
-                std::memcpy(&hb, &raw[t * 2], 2);
+                std::memcpy(&hb, &raw[e], 2);
                 const float r = fld == 0 ? mf[4 * t] : ms[4 * t + fld - 1];
                 v = half_bits_to_float(hb) + (r * poly_q_host(q, mf[4 * t + 1], mf[4 * t + 2], mf[4 * t + 3])) * w;
             }

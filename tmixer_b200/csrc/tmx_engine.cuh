@@ -42,13 +42,21 @@ namespace tmx {
 // Deterministic FP32 equilibrium polynomial (every operation rounded on its
 // own, no contraction): the FP16 form adds and subtracts this value when it
 // encodes and decodes populations, so both sides must produce the same bits.
-__device__ __forceinline__ float poly_q_rn(int q, float ux, float uy, float uz)
+// t = 1.5 |u|^2 is shared by the 19 directions; the FP16 form stores it
+// with the writer's moments so that readers need not recompute it.
+__device__ __forceinline__ float u2_term(float ux, float uy, float uz)
 {
-    const float u2 = __fadd_rn(__fadd_rn(__fmul_rn(ux, ux), __fmul_rn(uy, uy)), __fmul_rn(uz, uz));
-    const float t = __fmul_rn(1.5f, u2);
+    return __fmul_rn(1.5f, __fadd_rn(__fadd_rn(__fmul_rn(ux, ux), __fmul_rn(uy, uy)), __fmul_rn(uz, uz)));
+}
+__device__ __forceinline__ float poly_q_rn_t(int q, float ux, float uy, float uz, float t)
+{
     if (q == 0) return __fsub_rn(1.0f, t);
     const float eu = e_dot_u(q, ux, uy, uz);
     return __fadd_rn(__fsub_rn(__fadd_rn(1.0f, __fmul_rn(3.0f, eu)), t), __fmul_rn(__fmul_rn(4.5f, eu), eu));
+}
+__device__ __forceinline__ float poly_q_rn(int q, float ux, float uy, float uz)
+{
+    return poly_q_rn_t(q, ux, uy, uz, u2_term(ux, uy, uz));
 }
 
 // Plain form: FP64 storage and arithmetic, operation by operation as the
@@ -59,6 +67,11 @@ struct F64 {
     using S = double;
     static constexpr bool kMoments = false;
     static constexpr bool kOnePass = false;  // 76 FP64 values exceed the register budget
+    // structure of arrays: plane (fld, q) of ps values, nodes x-fastest
+    __host__ __device__ static long long off(int fld, int q, long long ps, long long g)
+    {
+        return (long long)(fld * 19 + q) * ps + g;
+    }
     __device__ static void poly(T ux, T uy, T uz, T (&p)[19]) { eq_poly(ux, uy, uz, p); }
     __device__ static bool tiny(T r) { return tiny_density(r); }
     __device__ static T feq(T r, T polyq, int q, bool tiny)
@@ -77,6 +90,24 @@ struct F32 {
     using S = float;
     static constexpr bool kMoments = false;
     static constexpr bool kOnePass = true;
+    // direction-major planes of ps nodes, the four fields of a node
+    // interleaved: one 16-byte access moves a node's direction q
+    __host__ __device__ static long long off(int fld, int q, long long ps, long long g)
+    {
+        return (((long long)q * ps + g) << 2) + fld;
+    }
+    __device__ static void load4(const S* p, T (&v)[4])
+    {
+        const float4 x = __ldg((const float4*)p);
+        v[0] = x.x;
+        v[1] = x.y;
+        v[2] = x.z;
+        v[3] = x.w;
+    }
+    __device__ static void encode4(S* p, const T (&v)[4], const T (&)[4])
+    {
+        *(float4*)p = make_float4(v[0], v[1], v[2], v[3]);
+    }
     __device__ static void poly(T ux, T uy, T uz, T (&p)[19]) { eq_poly(ux, uy, uz, p); }
     __device__ static bool tiny(T) { return false; }
     __device__ static T feq(T r, T polyq, int q, bool) { return r * polyq * (float)wq(q); }
@@ -87,7 +118,7 @@ struct F32 {
 
 // FP32 arithmetic; populations stored in FP16 as their non-equilibrium part
 // n_q = f_q - feq_q(rho, u) of the node that wrote them, next to that node's
-// FP32 moments M = {(rho, ux, uy, uz), (cA, cB, cC, 0)} (float4[2*ps]).  A
+// FP32 moments M = {(rho, ux, uy, uz), (cA, cB, cC, 1.5|u|^2)} (float4[2*ps]).  A
 // reader adds back feq_q of the writer's moments.  The stored quantity is of
 // the order of the gradients, so FP16 keeps about FP32 accuracy of f.
 struct F16 {
@@ -95,6 +126,29 @@ struct F16 {
     using S = __half;
     static constexpr bool kMoments = true;
     static constexpr bool kOnePass = true;
+    // layout of F32: one 8-byte access moves the four fields of (q, node)
+    __host__ __device__ static long long off(int fld, int q, long long ps, long long g)
+    {
+        return (((long long)q * ps + g) << 2) + fld;
+    }
+    __device__ static void load4(const S* p, T (&v)[4])
+    {
+        const uint2 x = __ldg((const uint2*)p);
+        const float2 lo = __half22float2(*(const __half2*)&x.x), hi = __half22float2(*(const __half2*)&x.y);
+        v[0] = lo.x;
+        v[1] = lo.y;
+        v[2] = hi.x;
+        v[3] = hi.y;
+    }
+    __device__ static void encode4(S* p, const T (&v)[4], const T (&feq)[4])
+    {
+        const __half2 lo = __floats2half2_rn(v[0] - feq[0], v[1] - feq[1]);
+        const __half2 hi = __floats2half2_rn(v[2] - feq[2], v[3] - feq[3]);
+        uint2 x;
+        x.x = *(const unsigned*)&lo;
+        x.y = *(const unsigned*)&hi;
+        *(uint2*)p = x;
+    }
     __device__ static void poly(T ux, T uy, T uz, T (&p)[19])
     {
 #pragma unroll
@@ -110,7 +164,8 @@ struct F16 {
             const float4 ms = __ldg(M + ps + src);
             r = fld == 1 ? ms.x : (fld == 2 ? ms.y : ms.z);
         }
-        return __half2float(__ldg(p)) + feq(r, poly_q_rn(q, mf.y, mf.z, mf.w), q, false);
+        const float t = __ldg(&M[ps + src].w);
+        return __half2float(__ldg(p)) + feq(r, poly_q_rn_t(q, mf.y, mf.z, mf.w, t), q, false);
     }
     __device__ static void encode(S* p, T v, T feq) { *p = __float2half_rn(v - feq); }
     __device__ static T raw(const S* p) { return __half2float(__ldg(p)); }
@@ -133,7 +188,6 @@ __device__ __forceinline__ void collide_store(typename PR::S* __restrict__ Pout,
 {
     using T = typename PR::T;
     const T c1 = T(P.c1[fld]), c2 = T(P.c2[fld]);
-    typename PR::S* out = Pout + (long long)fld * 19 * ps + g;
     const bool tiny = PR::tiny(r);
 #pragma unroll
     for (int q = 0; q < 19; q++) {
@@ -141,7 +195,41 @@ __device__ __forceinline__ void collide_store(typename PR::S* __restrict__ Pout,
         T v = f[q] * c1 + c2 * feq;
         if (fld == 1 || fld == 2) v = v - T(wq(q)) * rt;
         if (fld == 3) v = v + (T(wq(q)) * rt) * T(2);
-        PR::encode(out + (long long)q * ps, v, feq);
+        PR::encode(Pout + PR::off(fld, q, ps, g), v, feq);
+    }
+}
+
+// The four fields of a node at once, for the interleaved layouts: the same
+// arithmetic as collide_store on each field, one vector store per direction.
+template <class PR>
+__device__ __forceinline__ void collide_store4(typename PR::S* __restrict__ Pout, long long ps, int g,
+                                               const typename PR::T (&f)[19], const typename PR::T (&a)[19],
+                                               const typename PR::T (&b)[19], const typename PR::T (&c)[19],
+                                               typename PR::T rho, typename PR::T ca, typename PR::T cb,
+                                               typename PR::T cc, const typename PR::T (&poly)[19], const Phys& P,
+                                               typename PR::T rt)
+{
+    using T = typename PR::T;
+    const T r[4] = {rho, ca, cb, cc};
+    T c1[4], c2[4];
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+        c1[m] = T(P.c1[m]);
+        c2[m] = T(P.c2[m]);
+    }
+#pragma unroll
+    for (int q = 0; q < 19; q++) {
+        const T in[4] = {f[q], a[q], b[q], c[q]};
+        T v[4], feq[4];
+#pragma unroll
+        for (int m = 0; m < 4; m++) {
+            feq[m] = PR::feq(r[m], poly[q], q, false);
+            v[m] = in[m] * c1[m] + c2[m] * feq[m];
+        }
+        v[1] = v[1] - T(wq(q)) * rt;
+        v[2] = v[2] - T(wq(q)) * rt;
+        v[3] = v[3] + (T(wq(q)) * rt) * T(2);
+        PR::encode4(Pout + PR::off(0, q, ps, g), v, feq);
     }
 }
 
@@ -207,11 +295,10 @@ __device__ __forceinline__ void bulk_load(const typename PR::S* __restrict__ Pin
                                           long long ps, int fld, const Geom& G, int g, int i, int k, int sy, int sz,
                                           int iface, typename PR::T (&v)[19])
 {
-    const typename PR::S* base = Pin + (long long)fld * 19 * ps;
 #pragma unroll
     for (int q = 0; q < 19; q++) {
         const int src = bulk_src(G, g, i, k, sy, sz, iface, q);
-        v[q] = PR::decode(base + (long long)q * ps + src, fld, q, M, ps, src);
+        v[q] = PR::decode(Pin + PR::off(fld, q, ps, src), fld, q, M, ps, src);
     }
 }
 
@@ -280,7 +367,7 @@ __device__ __forceinline__ void bulk_node(const StepPtrs& X, const Geom& G, cons
     }
     if (PR::kMoments) {
         X.mcur[g] = make_float4((float)rho, (float)ux, (float)uy, (float)uz);
-        X.mcur[ps + g] = make_float4((float)ca, (float)cb, (float)cc, 0.f);
+        X.mcur[ps + g] = make_float4((float)ca, (float)cb, (float)cc, u2_term((float)ux, (float)uy, (float)uz));
     }
     if (write_macro) {
         double* Mac = X.mac;
@@ -316,20 +403,21 @@ __device__ __forceinline__ void bulk_node_lp(const StepPtrs& X, const Geom& G, c
 #pragma unroll
     for (int q = 0; q < 19; q++) {
         const int s = bulk_src(G, g, i, k, sy, sz, iface, q);
-        const typename PR::S* p = Pin + (long long)q * ps + s;
+        T raw[4];
+        PR::load4(Pin + PR::off(0, q, ps, s), raw);
         T e0 = T(0), e1 = T(0), e2 = T(0), e3 = T(0);
         if (PR::kMoments) {
             const float4 mf = __ldg(M + s), ms = __ldg(M + ps + s);
-            const float pq = poly_q_rn(q, mf.y, mf.z, mf.w);
+            const float pq = poly_q_rn_t(q, mf.y, mf.z, mf.w, ms.w);
             e0 = PR::feq(mf.x, pq, q, false);
             e1 = PR::feq(ms.x, pq, q, false);
             e2 = PR::feq(ms.y, pq, q, false);
             e3 = PR::feq(ms.z, pq, q, false);
         }
-        f[q] = PR::raw(p) + e0;
-        a[q] = PR::raw(p + 19 * ps) + e1;
-        bb[q] = PR::raw(p + 38 * ps) + e2;
-        c[q] = PR::raw(p + 57 * ps) + e3;
+        f[q] = raw[0] + e0;
+        a[q] = raw[1] + e1;
+        bb[q] = raw[2] + e2;
+        c[q] = raw[3] + e3;
     }
     const T rho = sum19(f);
     T sxm, sym, szm;
@@ -339,10 +427,7 @@ __device__ __forceinline__ void bulk_node_lp(const StepPtrs& X, const Geom& G, c
     PR::poly(ux, uy, uz, poly);
     const T ca = sum19(a), cb = sum19(bb), cc = sum19(c);
     const T rt = T(P.rateconst) * ca * cb;
-    collide_store<PR>(Pout, ps, g, 0, f, rho, poly, P, T(0));
-    collide_store<PR>(Pout, ps, g, 1, a, ca, poly, P, rt);
-    collide_store<PR>(Pout, ps, g, 2, bb, cb, poly, P, rt);
-    collide_store<PR>(Pout, ps, g, 3, c, cc, poly, P, rt);
+    collide_store4<PR>(Pout, ps, g, f, a, bb, c, rho, ca, cb, cc, poly, P, rt);
     if (b == 0 && j == 2 && (i == G.ia || i == G.ib)) {
         T* Rcur = (T*)X.rcur;
         Rcur[g] = rho;
@@ -352,7 +437,7 @@ __device__ __forceinline__ void bulk_node_lp(const StepPtrs& X, const Geom& G, c
     }
     if (PR::kMoments) {
         X.mcur[g] = make_float4((float)rho, (float)ux, (float)uy, (float)uz);
-        X.mcur[ps + g] = make_float4((float)ca, (float)cb, (float)cc, 0.f);
+        X.mcur[ps + g] = make_float4((float)ca, (float)cb, (float)cc, u2_term((float)ux, (float)uy, (float)uz));
     }
     if (write_macro) {
         double* Mac = X.mac;
@@ -386,7 +471,7 @@ struct BCtx {
 template <class PR>
 __device__ __forceinline__ typename PR::T own_fn(const BCtx<PR>& c, int fld, int q)
 {
-    return PR::decode(c.Pin + (long long)(fld * 19 + q) * c.ps + c.g, fld, q, c.M, c.ps, c.g);
+    return PR::decode(c.Pin + PR::off(fld, q, c.ps, c.g), fld, q, c.M, c.ps, c.g);
 }
 template <class PR>
 __device__ __forceinline__ typename PR::T rprev(const BCtx<PR>& c, int fld, int b, int i, int j, int k)
@@ -403,11 +488,10 @@ __device__ __forceinline__ void pull_node(const BCtx<PR>& c, int fld, int b, int
                                           typename PR::T (&v)[19])
 {
     using T = typename PR::T;
-    const typename PR::S* base = c.Pin + (long long)fld * 19 * c.ps;
 #pragma unroll
     for (int q = 0; q < 19; q++) {
         const int s = pull_src(*c.G, b, i, j, k, q);
-        v[q] = s >= 0 ? PR::decode(base + (long long)q * c.ps + s, fld, q, c.M, c.ps, s) : T(0);
+        v[q] = s >= 0 ? PR::decode(c.Pin + PR::off(fld, q, c.ps, s), fld, q, c.M, c.ps, s) : T(0);
     }
 }
 // the same sum as sum19 without two directions (the closures' "rho - (...)")
@@ -904,7 +988,7 @@ __device__ __forceinline__ void boundary_node(const StepPtrs& X, const int* __re
     Rcur[3 * ps + c.g] = cc;
     if (PR::kMoments) {
         X.mcur[c.g] = make_float4((float)rho, (float)ux, (float)uy, (float)uz);
-        X.mcur[ps + c.g] = make_float4((float)ca, (float)cb, (float)cc, 0.f);
+        X.mcur[ps + c.g] = make_float4((float)ca, (float)cb, (float)cc, u2_term((float)ux, (float)uy, (float)uz));
     }
     if (write_macro) {
         Mac[c.g] = rho;
@@ -917,6 +1001,17 @@ __device__ __forceinline__ void boundary_node(const StepPtrs& X, const int* __re
     }
 }
 
+// One interior node in the form's bulk scheme: one pass over the 76 values
+// for the interleaved layouts, field by field for FP64.
+template <class PR>
+__device__ __forceinline__ void bulk_any(const StepPtrs& X, const Geom& G, const Phys& P, int write_macro, int g)
+{
+    if constexpr (PR::kOnePass)
+        bulk_node_lp<PR>(X, G, P, write_macro, g);
+    else
+        bulk_node<PR>(X, G, P, write_macro, g);
+}
+
 // Kernel definitions for one precision policy; NAME is the kernel-name suffix.
 #define TMX_DEFINE_STEP_KERNELS(PR, NAME)                                                                         \
     __global__ void k_init_##NAME(StepPtrs X, Geom G, Phys P, double rho0)                                      \
@@ -927,10 +1022,7 @@ __device__ __forceinline__ void boundary_node(const StepPtrs& X, const int* __re
     __global__ void __launch_bounds__(256, 2) k_bulk_##NAME(StepPtrs X, Geom G, Phys P, int write_macro)        \
     {                                                                                                           \
         for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < G.nnodes; g += gridDim.x * blockDim.x)          \
-            if (PR::kOnePass)                                                                                   \
-                bulk_node_lp<PR>(X, G, P, write_macro, g);                                                      \
-            else                                                                                                \
-                bulk_node<PR>(X, G, P, write_macro, g);                                                         \
+            bulk_any<PR>(X, G, P, write_macro, g);                                                              \
     }                                                                                                           \
     __global__ void __launch_bounds__(kBoundaryThreads) k_bfaces_##NAME(                                       \
         StepPtrs X, const int* bnode, const unsigned char* bcls, int nb, Geom G, Phys P, int write_macro)       \
