@@ -333,12 +333,12 @@ int enqueue_step(tmx_handle* h, int cur, int write_macro, cudaEvent_t* ev)
     TMX_CK(cudaStreamWaitEvent(h->aux2, h->fork, 0));
     if (ev) TMX_CK(cudaEventRecord(ev[2], h->aux));
     const int nf = h->nface, ne = h->nb - h->nface;
-    const int bt = tmx::kBoundaryThreadsHost;
+    const int bt = tmx::kBoundaryThreadsHost, nl = tmx::kBoundaryLanesHost;  // nl threads per node
     if (nf > 0)
-        h->K->faces<<<(nf + bt - 1) / bt, bt, 0, h->aux>>>(X, h->bnode, h->bcls, nf, G, h->P, write_macro);
+        h->K->faces<<<(nl * nf + bt - 1) / bt, bt, 0, h->aux>>>(X, h->bnode, h->bcls, nf, G, h->P, write_macro);
     if (ne > 0)
-        h->K->edges<<<(ne + bt - 1) / bt, bt, 0, h->aux2>>>(X, h->bnode + nf, h->bcls + nf, ne, G, h->P,
-                                                            write_macro);
+        h->K->edges<<<(nl * ne + bt - 1) / bt, bt, 0, h->aux2>>>(X, h->bnode + nf, h->bcls + nf, ne, G, h->P,
+                                                                 write_macro);
     TMX_CK(cudaEventRecord(h->join2, h->aux2));
     if (ev) {  // the boundary time spans both boundary kernels
         TMX_CK(cudaStreamWaitEvent(h->aux, h->join2, 0));

@@ -55,17 +55,23 @@ __host__ __device__ inline bool is_boundary(const Geom& G, int b, int i, int j, 
     return i == 1 || i == G.mnx || j == 1;
 }
 
+// Per-box sizes by selection rather than by indexing: a kernel argument
+// indexed with a run-time value would be copied to local memory.
+__host__ __device__ inline int box_nx(const Geom& G, int b) { return b ? G.nx[1] : G.nx[0]; }
+__host__ __device__ inline int box_ny(const Geom& G, int b) { return b ? G.ny[1] : G.ny[0]; }
+__host__ __device__ inline int box_base(const Geom& G, int b) { return b ? G.base[1] : G.base[0]; }
+
 __host__ __device__ inline int node_index(const Geom& G, int b, int i, int j, int k)
 {
-    return G.base[b] + ((k - 1) * G.ny[b] + (j - 1)) * G.nx[b] + (i - 1);
+    return box_base(G, b) + ((k - 1) * box_ny(G, b) + (j - 1)) * box_nx(G, b) + (i - 1);
 }
 
 // box and 1-based coordinates of node g
 __host__ __device__ inline void decode(const Geom& G, int g, int& b, int& i, int& j, int& k)
 {
     b = g >= G.base[1];
-    const int l = g - G.base[b];
-    const int nx = G.nx[b], ny = G.ny[b];
+    const int l = g - box_base(G, b);
+    const int nx = box_nx(G, b), ny = box_ny(G, b);
     i = l % nx + 1;
     const int t = l / nx;
     j = t % ny + 1;
@@ -90,7 +96,7 @@ __host__ __device__ inline int pull_src(const Geom& G, int b, int i, int j, int 
         si = i + G.ia - 1 - EX(q);
         sj = 1;
     }
-    if (si < 1 || si > G.nx[sb] || sj < 1 || sj > G.ny[sb] || sk < 1 || sk > G.nz) return -1;
+    if (si < 1 || si > box_nx(G, sb) || sj < 1 || sj > box_ny(G, sb) || sk < 1 || sk > G.nz) return -1;
     return node_index(G, sb, si, sj, sk);
 }
 

@@ -176,6 +176,16 @@ struct F16 {
 // per-node physics: equilibrium -> collision -> store
 // ---------------------------------------------------------------------------
 
+// Per-field constants by selection (fld may be a run-time value; see box_nx).
+__device__ __forceinline__ double pick_field(const double (&a)[4], int fld)
+{
+    return fld == 0 ? a[0] : (fld == 1 ? a[1] : (fld == 2 ? a[2] : a[3]));
+}
+__device__ __forceinline__ double pick_species(const double (&cin)[3][2], int fld, int n)
+{
+    return fld == 1 ? cin[0][n] : (fld == 2 ? cin[1][n] : cin[2][n]);
+}
+
 // Collide one field given its populations f, density r and the shared
 // equilibrium polynomial, and store the result.  The reaction source of
 // Tmixer.cpp:9697-9761: species A and B (fld 1, 2) lose (w_q*rt)*1.0, C gains
@@ -187,7 +197,7 @@ __device__ __forceinline__ void collide_store(typename PR::S* __restrict__ Pout,
                                               const typename PR::T (&poly)[19], const Phys& P, typename PR::T rt)
 {
     using T = typename PR::T;
-    const T c1 = T(P.c1[fld]), c2 = T(P.c2[fld]);
+    const T c1 = T(pick_field(P.c1, fld)), c2 = T(pick_field(P.c2, fld));
     const bool tiny = PR::tiny(r);
 #pragma unroll
     for (int q = 0; q < 19; q++) {
@@ -315,7 +325,7 @@ __device__ __forceinline__ void bulk_node(const StepPtrs& X, const Geom& G, cons
     int b, i, j, k;
     decode(G, g, b, i, j, k);
     if (is_boundary(G, b, i, j, k)) return;
-    const int sy = G.nx[b], sz = G.nx[b] * G.ny[b];
+    const int sy = box_nx(G, b), sz = box_nx(G, b) * box_ny(G, b);
     const int iface = (b == 0 && j == 1) ? 1 : ((b == 1 && j == G.mny) ? 2 : 0);
 
     // flow: moments, equilibrium polynomial (shared by all four fields: they
@@ -396,7 +406,7 @@ __device__ __forceinline__ void bulk_node_lp(const StepPtrs& X, const Geom& G, c
     int b, i, j, k;
     decode(G, g, b, i, j, k);
     if (is_boundary(G, b, i, j, k)) return;
-    const int sy = G.nx[b], sz = G.nx[b] * G.ny[b];
+    const int sy = box_nx(G, b), sz = box_nx(G, b) * box_ny(G, b);
     const int iface = (b == 0 && j == 1) ? 1 : ((b == 1 && j == G.mny) ? 2 : 0);
 
     T f[19], a[19], bb[19], c[19];
@@ -600,7 +610,7 @@ __device__ __forceinline__ void closure_face(const BCtx<PR>& c, int cls, int fld
             v[1] = v[3] + (r * U) / T(3);
             v[7] = v[9] - (A + B); v[10] = v[8] - (A - B); v[11] = v[13] - (A + C); v[14] = v[12] - (A - C);
         } else {
-            const T cin = c.P->cin[fld - 1][0];
+            const T cin = pick_species(c.P->cin, fld, 0);
             v[1] = -v[3] + T(2.0 / 18.0) * cin;
             v[7] = -v[9] + T(2.0 / 36.0) * cin;
             v[10] = -v[8] + T(2.0 / 36.0) * cin;
@@ -619,7 +629,7 @@ __device__ __forceinline__ void closure_face(const BCtx<PR>& c, int cls, int fld
             v[3] = v[1] - (r * (U)) / T(3);
             v[9] = v[7] + (A + B); v[8] = v[10] + (A - B); v[13] = v[11] + (A + C); v[12] = v[14] + (A - C);
         } else {
-            const T cin = c.P->cin[fld - 1][1];
+            const T cin = pick_species(c.P->cin, fld, 1);
             v[3] = -v[1] + T(2.0 / 18.0) * cin;
             v[9] = -v[7] + T(2.0 / 36.0) * cin;
             v[8] = -v[10] + T(2.0 / 36.0) * cin;
@@ -906,22 +916,28 @@ __device__ __forceinline__ void closed_pull(const BCtx<PR>& c, int cls, int fld,
 }
 
 // ---------------------------------------------------------------------------
-// boundary nodes: one thread per node of a compact, class-sorted list; FACES
-// selects the list of inlet/outlet/wall-face nodes or of edge/corner nodes.
-// The closed species A and B populations wait in shared memory while the
-// reaction term (which needs both densities) is formed.
+// boundary nodes of a compact, class-sorted list, four threads per node: lane
+// fld (0 flow, 1 A, 2 B, 3 C) pulls, closes and collides its own field.  Every
+// closure reads only its own field, so the lanes need each other only for
+// the moments: the flow lane's density and velocity and the species
+// densities (for the reaction term), passed by warp shuffles.  FACES selects
+// the list of inlet/outlet/wall-face nodes or of edge/corner nodes.
 // ---------------------------------------------------------------------------
 constexpr int kBoundaryThreads = 128;
+constexpr int kBoundaryLanes = 4;
 
 template <class PR, bool FACES>
 __device__ __forceinline__ void boundary_node(const StepPtrs& X, const int* __restrict__ bnode,
                                               const unsigned char* __restrict__ bcls, int nb, const Geom& G,
-                                              const Phys& P, int write_macro,
-                                              typename PR::T (*stash)[19][kBoundaryThreads])
+                                              const Phys& P, int write_macro)
 {
     using T = typename PR::T;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = gt >> 2, fld = gt & 3;
+    // the four lanes of a node share one warp; whole nodes drop out together
+    const unsigned mask = __ballot_sync(0xffffffffu, t < nb);
     if (t >= nb) return;
+    const int lead = (threadIdx.x & 31) & ~3;
     typename PR::S* __restrict__ Pout = (typename PR::S*)X.pout;
     T* __restrict__ Rcur = (T*)X.rcur;
     double* __restrict__ Mac = X.mac;
@@ -938,66 +954,45 @@ __device__ __forceinline__ void boundary_node(const StepPtrs& X, const int* __re
     decode(G, c.g, c.b, c.i, c.j, c.k);
     const int cls = bcls[t];
     const long long ps = G.ps;
-    const bool outlet = c.b == 1 && c.j == 1;
-    const int tx = threadIdx.x;
 
-    T poly[19];
-    T rho, ux, uy, uz;
-    {
-        T f[19];
-        closed_pull<PR, FACES>(c, cls, 0, f);
+    T v[19];
+    closed_pull<PR, FACES>(c, cls, fld, v);
+    T r = sum19(v);
+    T ux = T(0), uy = T(0), uz = T(0);
+    if (fld == 0) {
         // the outlet row's density is pinned to rho_out (Tmixer.cpp:9575-9582)
-        rho = outlet ? T(P.rho_out) : sum19(f);
+        if (c.b == 1 && c.j == 1) r = T(P.rho_out);
         T sxm, sym, szm;
-        momentum(f, sxm, sym, szm);
-        ux = sxm / rho;
-        uy = sym / rho;
-        uz = szm / rho;
-        PR::poly(ux, uy, uz, poly);
-        collide_store<PR>(Pout, ps, c.g, 0, f, rho, poly, P, T(0));
+        momentum(v, sxm, sym, szm);
+        ux = sxm / r;
+        uy = sym / r;
+        uz = szm / r;
     }
-    T ca, cb, cc;
-    {
-        T v[19];
-        closed_pull<PR, FACES>(c, cls, 1, v);
-        ca = sum19(v);
-#pragma unroll
-        for (int q = 0; q < 19; q++) stash[0][q][tx] = v[q];
-        closed_pull<PR, FACES>(c, cls, 2, v);
-        cb = sum19(v);
-#pragma unroll
-        for (int q = 0; q < 19; q++) stash[1][q][tx] = v[q];
-    }
-    const T rt = T(P.rateconst) * ca * cb;
-    {
-        T v[19];
-#pragma unroll
-        for (int q = 0; q < 19; q++) v[q] = stash[0][q][tx];
-        collide_store<PR>(Pout, ps, c.g, 1, v, ca, poly, P, rt);
-#pragma unroll
-        for (int q = 0; q < 19; q++) v[q] = stash[1][q][tx];
-        collide_store<PR>(Pout, ps, c.g, 2, v, cb, poly, P, rt);
-        closed_pull<PR, FACES>(c, cls, 3, v);
-        cc = sum19(v);
-        collide_store<PR>(Pout, ps, c.g, 3, v, cc, poly, P, rt);
-    }
+    ux = __shfl_sync(mask, ux, lead);
+    uy = __shfl_sync(mask, uy, lead);
+    uz = __shfl_sync(mask, uz, lead);
+    const T rho = __shfl_sync(mask, r, lead);
+    const T ca = __shfl_sync(mask, r, lead + 1);
+    const T cb = __shfl_sync(mask, r, lead + 2);
+    const T cc = __shfl_sync(mask, r, lead + 3);
+    T poly[19];
+    PR::poly(ux, uy, uz, poly);
+    const T rt = fld == 0 ? T(0) : T(P.rateconst) * ca * cb;
+    collide_store<PR>(Pout, ps, c.g, fld, v, r, poly, P, rt);
 
-    Rcur[c.g] = rho;
-    Rcur[ps + c.g] = ca;
-    Rcur[2 * ps + c.g] = cb;
-    Rcur[3 * ps + c.g] = cc;
+    Rcur[fld * ps + c.g] = r;
     if (PR::kMoments) {
-        X.mcur[c.g] = make_float4((float)rho, (float)ux, (float)uy, (float)uz);
-        X.mcur[ps + c.g] = make_float4((float)ca, (float)cb, (float)cc, u2_term((float)ux, (float)uy, (float)uz));
+        if (fld == 0) X.mcur[c.g] = make_float4((float)rho, (float)ux, (float)uy, (float)uz);
+        if (fld == 1)
+            X.mcur[ps + c.g] = make_float4((float)ca, (float)cb, (float)cc, u2_term((float)ux, (float)uy, (float)uz));
     }
     if (write_macro) {
-        Mac[c.g] = rho;
-        Mac[ps + c.g] = ux;
-        Mac[2 * ps + c.g] = uy;
-        Mac[3 * ps + c.g] = uz;
-        Mac[4 * ps + c.g] = ca;
-        Mac[5 * ps + c.g] = cb;
-        Mac[6 * ps + c.g] = cc;
+        Mac[(fld == 0 ? 0 : 3 + fld) * ps + c.g] = r;
+        if (fld == 0) {
+            Mac[ps + c.g] = ux;
+            Mac[2 * ps + c.g] = uy;
+            Mac[3 * ps + c.g] = uz;
+        }
     }
 }
 
@@ -1027,14 +1022,12 @@ __device__ __forceinline__ void bulk_any(const StepPtrs& X, const Geom& G, const
     __global__ void __launch_bounds__(kBoundaryThreads) k_bfaces_##NAME(                                       \
         StepPtrs X, const int* bnode, const unsigned char* bcls, int nb, Geom G, Phys P, int write_macro)       \
     {                                                                                                           \
-        __shared__ PR::T stash[2][19][kBoundaryThreads];                                                        \
-        boundary_node<PR, true>(X, bnode, bcls, nb, G, P, write_macro, stash);                                  \
+        boundary_node<PR, true>(X, bnode, bcls, nb, G, P, write_macro);                                         \
     }                                                                                                           \
     __global__ void __launch_bounds__(kBoundaryThreads) k_bedges_##NAME(                                       \
         StepPtrs X, const int* bnode, const unsigned char* bcls, int nb, Geom G, Phys P, int write_macro)       \
     {                                                                                                           \
-        __shared__ PR::T stash[2][19][kBoundaryThreads];                                                        \
-        boundary_node<PR, false>(X, bnode, bcls, nb, G, P, write_macro, stash);                                 \
+        boundary_node<PR, false>(X, bnode, bcls, nb, G, P, write_macro);                                        \
     }
 
 }  // namespace tmx

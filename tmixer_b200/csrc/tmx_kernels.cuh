@@ -23,6 +23,7 @@ struct StepPtrs {
 };
 
 constexpr int kBoundaryThreadsHost = 128;  // block size of the boundary kernels
+constexpr int kBoundaryLanesHost = 4;      // threads per boundary node (one per field)
 
 #define TMX_DECLARE_STEP_KERNELS(NAME)                                                                          \
     __global__ void k_init_##NAME(StepPtrs X, Geom G, Phys P, double rho0);                                     \
