@@ -188,6 +188,78 @@ int tmx_counts(const tmx_handle *h, long long out[4]);
  * (Tmixer.cpp:1083-1366). */
 void tmx_destroy(tmx_handle *h);
 
+/* ------------------------------------------------------------------------
+ * Batched engine: many mixers of uneven size and parameters stepped together,
+ * each step one launch per kernel kind over all of them (a persistent bulk
+ * kernel over a concatenated cell-block list, and persistent boundary kernels
+ * over the concatenated boundary-node lists), with the step captured as a
+ * CUDA graph.  The reference runs one case per process and has no
+ * counterpart for any of these functions.  One batch is used from one host
+ * thread at a time.
+ * ------------------------------------------------------------------------ */
+typedef struct tmx_batch tmx_batch;
+
+/* Device bytes one mixer of this case takes in a batch. */
+int tmx_batch_footprint(const tmx_case *c, long long *bytes);
+
+/* Create a batch of the given precision (every case added must have it)
+ * whose mixers share one device arena of budget_bytes, allocated here. */
+int tmx_batch_create(int precision, long long budget_bytes, int device, tmx_batch **out);
+
+/* Admit one mixer: carve its state from the arena (TMX_E_NOMEM if no free
+ * range of its footprint is left), compute its inlet profiles and initial
+ * state (as tmx_init does), and return its slot number.  It joins the next
+ * step of the batch. */
+int tmx_batch_add(tmx_batch *b, const tmx_case *c, int *slot);
+
+/* Retire a mixer and return its range to the arena; the slot number may be
+ * reused by a later tmx_batch_add. */
+int tmx_batch_remove(tmx_batch *b, int slot);
+
+/* Advance every mixer of the batch by nsteps steps (asynchronous).  With
+ * write_macro_last the last step also writes the macroscopic fields that
+ * tmx_batch_fields and tmx_batch_outlet_im read. */
+int tmx_batch_step(tmx_batch *b, int nsteps, int write_macro_last);
+
+/* Wait for the batch's queued work. */
+int tmx_batch_sync(tmx_batch *b);
+
+/* Slot numbers in use (at most cap written to slots; *n = how many there are). */
+int tmx_batch_slots(const tmx_batch *b, int *slots, int cap, int *n);
+
+/* Steps taken by the mixer in a slot since it was admitted (-1 if unused). */
+long long tmx_batch_slot_steps(const tmx_batch *b, int slot);
+
+/* Outlet mixing quality of n mixers: I_A, I_B, I_C of mixing row 1, as the
+ * first row of tmx_mixing, into im_out[3*e .. 3*e+2] for slots[e].  Reads the
+ * macroscopic fields of the last step that wrote them; waits for the result. */
+int tmx_batch_outlet_im(tmx_batch *b, const int *slots, int n, double *im_out);
+
+/* One macroscopic field of one box of one mixer, as tmx_fields. */
+int tmx_batch_fields(tmx_batch *b, int slot, int box, int field, double *host_out);
+
+/* out[0] mixers, out[1] their fluid nodes, out[2] arena bytes, out[3] free
+ * arena bytes, out[4] bulk threads per block, out[5] nodes per cell block,
+ * out[6] batch steps taken, out[7] bytes of the batch's work lists. */
+int tmx_batch_info(const tmx_batch *b, long long out[8]);
+
+/* Set the bulk kernel's launch shape: threads per block (128, 256 or 512) and
+ * nodes per cell block (a multiple of it). */
+int tmx_batch_set_shape(tmx_batch *b, int threads, int cells);
+
+/* Autotune the launch shape on the batch's current mixers: time
+ * steps_per_trial steps of every (threads, cells) choice, keep the fastest,
+ * then start every mixer again from its initial state.  Returns the choice
+ * and its time per step (ms). */
+int tmx_batch_tune(tmx_batch *b, int steps_per_trial, int *threads_out, int *cells_out, double *ms_out);
+
+/* Run nsteps steps between two CUDA events on the batch's stream and return
+ * the elapsed device time (ms). */
+int tmx_batch_time_steps(tmx_batch *b, int nsteps, double *ms);
+
+/* Free the batch, its arena and its mixers. */
+void tmx_batch_destroy(tmx_batch *b);
+
 #ifdef __cplusplus
 }
 #endif

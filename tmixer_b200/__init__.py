@@ -88,6 +88,24 @@ def lib() -> ctypes.CDLL:
     L.tmx_time_steps.argtypes = [vp, ip, P(dp)]
     L.tmx_destroy.argtypes = [vp]
     L.tmx_destroy.restype = None
+    LL = ctypes.c_longlong
+    L.tmx_batch_footprint.argtypes = [P(_CCase), P(LL)]
+    L.tmx_batch_create.argtypes = [ip, LL, ip, P(vp)]
+    L.tmx_batch_add.argtypes = [vp, P(_CCase), P(ip)]
+    L.tmx_batch_remove.argtypes = [vp, ip]
+    L.tmx_batch_step.argtypes = [vp, ip, ip]
+    L.tmx_batch_sync.argtypes = [vp]
+    L.tmx_batch_slots.argtypes = [vp, P(ip), ip, P(ip)]
+    L.tmx_batch_slot_steps.argtypes = [vp, ip]
+    L.tmx_batch_slot_steps.restype = LL
+    L.tmx_batch_outlet_im.argtypes = [vp, P(ip), ip, vp]
+    L.tmx_batch_fields.argtypes = [vp, ip, ip, ip, vp]
+    L.tmx_batch_info.argtypes = [vp, P(LL)]
+    L.tmx_batch_set_shape.argtypes = [vp, ip, ip]
+    L.tmx_batch_tune.argtypes = [vp, ip, P(ip), P(ip), P(dp)]
+    L.tmx_batch_time_steps.argtypes = [vp, ip, P(dp)]
+    L.tmx_batch_destroy.argtypes = [vp]
+    L.tmx_batch_destroy.restype = None
     if L.tmx_abi_version() != ABI_VERSION:
         raise RuntimeError("libtmx.so ABI %d, expected %d" % (L.tmx_abi_version(), ABI_VERSION))
     _lib = L
@@ -294,5 +312,106 @@ class Solver:
         return dict(nodes=o[0], interior=o[1], boundary=o[2], device_bytes=o[3])
 
 
-__all__ = ["CaseSpec", "Solver", "TmxError", "FIELDS", "TMX_FP64", "TMX_FP32", "TMX_FP16", "PRECISIONS",
+class Batch:
+    """Many mixers of one precision stepped together (tmx_batch_*): one
+    launch per kernel kind per step over all of them, state carved from one
+    device arena of ``budget`` bytes."""
+
+    def __init__(self, precision: int = TMX_FP16, budget: int = 1 << 30, device: int = 0):
+        self.precision = int(precision)
+        self._b = ctypes.c_void_p()
+        self.specs = {}
+        _check(lib().tmx_batch_create(self.precision, ctypes.c_longlong(int(budget)), int(device),
+                                      ctypes.byref(self._b)))
+
+    @staticmethod
+    def footprint(spec: CaseSpec) -> int:
+        c = spec.to_c()
+        n = ctypes.c_longlong()
+        _check(lib().tmx_batch_footprint(ctypes.byref(c), ctypes.byref(n)))
+        return int(n.value)
+
+    def add(self, spec: CaseSpec) -> int:
+        c = spec.to_c()
+        slot = ctypes.c_int()
+        _check(lib().tmx_batch_add(self._b, ctypes.byref(c), ctypes.byref(slot)))
+        self.specs[slot.value] = spec
+        return slot.value
+
+    def remove(self, slot: int) -> None:
+        _check(lib().tmx_batch_remove(self._b, int(slot)))
+        self.specs.pop(int(slot), None)
+
+    def step(self, n: int = 1, write_macro: bool = True) -> "Batch":
+        _check(lib().tmx_batch_step(self._b, int(n), 1 if write_macro else 0))
+        return self
+
+    def sync(self) -> None:
+        _check(lib().tmx_batch_sync(self._b))
+
+    def slots(self) -> list:
+        n = ctypes.c_int()
+        _check(lib().tmx_batch_slots(self._b, None, 0, ctypes.byref(n)))
+        arr = (ctypes.c_int * max(1, n.value))()
+        _check(lib().tmx_batch_slots(self._b, arr, n.value, ctypes.byref(n)))
+        return list(arr[:n.value])
+
+    def slot_steps(self, slot: int) -> int:
+        return int(lib().tmx_batch_slot_steps(self._b, int(slot)))
+
+    def outlet_im(self, slots=None) -> np.ndarray:
+        """(len(slots), 3) outlet I_A, I_B, I_C after the last step that
+        wrote the macroscopic fields."""
+        slots = self.slots() if slots is None else list(slots)
+        out = np.empty((len(slots), 3), dtype=np.float64)
+        arr = (ctypes.c_int * max(1, len(slots)))(*slots)
+        _check(lib().tmx_batch_outlet_im(self._b, arr, len(slots), out.ctypes.data))
+        return out
+
+    def field(self, slot: int, box: int, name: str) -> np.ndarray:
+        s = self.specs[int(slot)]
+        shape = (s.inx, s.iny, s.nz) if box == 0 else (s.mnx, s.mny, s.nz)
+        out = np.empty(shape, dtype=np.float64)
+        _check(lib().tmx_batch_fields(self._b, int(slot), int(box), FIELDS.index(name), out.ctypes.data))
+        return out
+
+    def info(self) -> dict:
+        o = (ctypes.c_longlong * 8)()
+        _check(lib().tmx_batch_info(self._b, o))
+        return dict(mixers=o[0], nodes=o[1], arena_bytes=o[2], free_bytes=o[3], threads=o[4], cells=o[5],
+                    steps=o[6], table_bytes=o[7])
+
+    def set_shape(self, threads: int, cells: int) -> None:
+        _check(lib().tmx_batch_set_shape(self._b, int(threads), int(cells)))
+
+    def tune(self, steps_per_trial: int = 10) -> dict:
+        t, c, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        _check(lib().tmx_batch_tune(self._b, int(steps_per_trial), ctypes.byref(t), ctypes.byref(c),
+                                    ctypes.byref(ms)))
+        return dict(threads=t.value, cells=c.value, ms_per_step=ms.value)
+
+    def time_steps(self, n: int) -> float:
+        ms = ctypes.c_double()
+        _check(lib().tmx_batch_time_steps(self._b, int(n), ctypes.byref(ms)))
+        return ms.value
+
+    def close(self) -> None:
+        if self._b:
+            lib().tmx_batch_destroy(self._b)
+            self._b = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+__all__ = ["CaseSpec", "Solver", "Batch", "TmxError", "FIELDS", "TMX_FP64", "TMX_FP32", "TMX_FP16", "PRECISIONS",
            "reference_case", "w_layout", "lib"]

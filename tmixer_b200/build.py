@@ -20,7 +20,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC"]
 # per-source contraction: the FP64 kernels and the host code keep every
 # operation separately rounded; the reduced-precision kernels may fuse
-SOURCES = {"tmx_kernels.cu": ["--fmad=false"], "tmx_api.cu": ["--fmad=false"], "tmx_kernels_lp.cu": ["--fmad=true"]}
+SOURCES = {"tmx_kernels.cu": ["--fmad=false"], "tmx_api.cu": ["--fmad=false"], "tmx_kernels_lp.cu": ["--fmad=true"],
+           "tmx_batch.cu": ["--fmad=false"]}
 OBJDIR = os.path.join(PKG, "_build")
 
 

@@ -17,14 +17,18 @@
 
 #include "../../include/tmx.h"
 #include "tmx_classes.h"
+#include "tmx_host.h"
 #include "tmx_kernels.cuh"
 
 using tmx::Geom;
 using tmx::Phys;
+using namespace tmx_host;
 
-namespace {
+namespace tmx_host {
 
 thread_local std::string g_err;
+
+const char* last_error() { return g_err.c_str(); }
 
 int fail(int code, const char* fmt, ...)
 {
@@ -37,14 +41,7 @@ int fail(int code, const char* fmt, ...)
     return code;
 }
 
-#define TMX_CK(call)                                                                                    \
-    do {                                                                                                \
-        cudaError_t e_ = (call);                                                                        \
-        if (e_ != cudaSuccess) return fail(TMX_E_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), \
-                                           __FILE__, __LINE__);                                         \
-    } while (0)
-
-}  // namespace
+}  // namespace tmx_host
 
 struct tmx_handle {
     tmx_case c;
@@ -82,24 +79,13 @@ struct tmx_handle {
     const struct StepKernels* K = nullptr;
 };
 
-// the step kernels of one form
-struct StepKernels {
-    void (*init)(tmx::StepPtrs, Geom, Phys, double);
-    void (*bulk)(tmx::StepPtrs, Geom, Phys, int);
-    void (*faces)(tmx::StepPtrs, const int*, const unsigned char*, int, Geom, Phys, int);
-    void (*edges)(tmx::StepPtrs, const int*, const unsigned char*, int, Geom, Phys, int);
-    int sbytes, tbytes;
-    bool moments;  // the form stores per-node FP32 moments next to the populations
-};
-static const StepKernels kForms[3] = {
+const StepKernels tmx_host::kForms[3] = {
     {tmx::k_init_f64, tmx::k_bulk_f64, tmx::k_bfaces_f64, tmx::k_bedges_f64, 8, 8, false},
     {tmx::k_init_f32, tmx::k_bulk_f32, tmx::k_bfaces_f32, tmx::k_bedges_f32, 4, 4, false},
     {tmx::k_init_f16, tmx::k_bulk_f16, tmx::k_bfaces_f16, tmx::k_bedges_f16, 2, 4, true},
 };
 
-namespace {
-
-constexpr int kSumBlocks = 592;
+namespace tmx_host {
 
 // The FP16 form's equilibrium polynomial (tmx_engine.cuh poly_q_rn), in host
 // single precision with every operation rounded on its own.
@@ -232,11 +218,10 @@ int classify(const Geom& G, int b, int i, int j, int k)
 // the same loop nesting and operation order), scaled to mean umean, then
 // shifted one node down in z (Uin1) and, negated, one node up (Uin2), with
 // Uin1[.][1] and Uin2[.][nz] zeroed.
-void inlet_profile(const tmx_case& c, std::vector<double>& U1, std::vector<double>& U2)
+void inlet_series(int iny, int nz, std::vector<double>& U1, double& average)
 {
-    const int iny = c.iny, nz = c.nz, W = nz + 3;
+    const int W = nz + 3;
     U1.assign((size_t)(iny + 3) * W, 0.0);
-    U2.assign((size_t)(iny + 3) * W, 0.0);
     auto at = [W](std::vector<double>& a, int j, int k) -> double& { return a[(size_t)j * W + k]; };
     const double pi = 3.14159265358979323846;
     const double d = ((nz - 1.0) / 2.0);
@@ -261,7 +246,16 @@ void inlet_profile(const tmx_case& c, std::vector<double>& U1, std::vector<doubl
     double sum = 0;
     for (int i = 1; i <= iny; i++)
         for (int j = 1; j <= nz; j++) sum += at(U1, i, j);
-    const double average = sum / ((iny) * (nz));
+    average = sum / ((iny) * (nz));
+}
+
+void inlet_scale(const tmx_case& c, const std::vector<double>& raw, double average, std::vector<double>& U1,
+                 std::vector<double>& U2)
+{
+    const int iny = c.iny, nz = c.nz, W = nz + 3;
+    U1 = raw;
+    U2.assign((size_t)(iny + 3) * W, 0.0);
+    auto at = [W](std::vector<double>& a, int j, int k) -> double& { return a[(size_t)j * W + k]; };
     for (int i = 1; i <= iny; i++)
         for (int j = 1; j <= nz; j++) at(U1, i, j) = at(U1, i, j) * (c.umean / average);
     for (int j = 0; j < iny; j++)
@@ -274,6 +268,47 @@ void inlet_profile(const tmx_case& c, std::vector<double>& U1, std::vector<doubl
         at(U2, i, nz) = 0;
     }
 }
+
+void inlet_profile(const tmx_case& c, std::vector<double>& U1, std::vector<double>& U2)
+{
+    std::vector<double> raw;
+    double average;
+    inlet_series(c.iny, c.nz, raw, average);
+    inlet_scale(c, raw, average, U1, U2);
+}
+
+int boundary_list(const Geom& G, std::vector<int>& nodes, std::vector<unsigned char>& cls, int& nface,
+                  std::vector<int>* class_count)
+{
+    std::vector<std::pair<int, int>> bl;
+    bl.reserve((size_t)boundary_count(G));
+    if (class_count) class_count->assign(tmx::K_NCLASSES, 0);
+    for (int b = 0; b < 2; b++)
+        for (int i = 1; i <= G.nx[b]; i++)
+            for (int j = 1; j <= G.ny[b]; j++)
+                for (int k = 1; k <= G.nz; k++) {
+                    if (!tmx::is_boundary(G, b, i, j, k)) continue;
+                    const int c = classify(G, b, i, j, k);
+                    if (c < 0) return fail(TMX_E_INVALID, "internal: boundary node (%d,%d,%d,%d) has no class", b, i, j, k);
+                    // faces first, then edges and corners; by class, then node
+                    bl.emplace_back((tmx::is_face_class(c) ? 0 : 256) + c, tmx::node_index(G, b, i, j, k));
+                    if (class_count) (*class_count)[c]++;
+                }
+    std::sort(bl.begin(), bl.end());
+    nodes.resize(bl.size());
+    cls.resize(bl.size());
+    nface = 0;
+    for (size_t t = 0; t < bl.size(); t++) {
+        cls[t] = (unsigned char)(bl[t].first & 255);
+        nodes[t] = bl[t].second;
+        if (bl[t].first < 256) nface++;
+    }
+    return TMX_OK;
+}
+
+}  // namespace tmx_host
+
+namespace {
 
 void free_all(tmx_handle* h)
 {
@@ -394,11 +429,37 @@ int timed_step(tmx_handle* h, int write_macro, cudaEvent_t* ev)
 
 }  // namespace
 
+namespace tmx_host {
+
+int check_case(const tmx_case& cc)
+{
+    const tmx_case* c = &cc;
+    if (c->inx < 3 || c->iny < 3 || c->nz < 3 || c->mnx < 3 || c->mny < 3)
+        return fail(TMX_E_INVALID, "every box size must be >= 3 (inx=%d iny=%d nz=%d mnx=%d mny=%d)", c->inx, c->iny,
+                    c->nz, c->mnx, c->mny);
+    if (c->ia < 2 || c->ia + c->mnx - 1 > c->inx - 1)
+        return fail(TMX_E_INVALID, "opening columns ia=%d..ib=%d must lie within 2..inx-1=%d", c->ia,
+                    c->ia + c->mnx - 1, c->inx - 1);
+    const double t[4] = {c->tau, c->tau_a, c->tau_b, c->tau_c};
+    for (double v : t)
+        if (!(v > 0.5) || !std::isfinite(v)) return fail(TMX_E_INVALID, "relaxation times must be finite and > 0.5");
+    if (!std::isfinite(c->rho0) || !(c->rho0 > 0) || !std::isfinite(c->rho_out) || !(c->rho_out > 0))
+        return fail(TMX_E_INVALID, "rho0 and rho_out must be finite and positive");
+    if (!std::isfinite(c->umean) || !std::isfinite(c->rateconst)) return fail(TMX_E_INVALID, "non-finite parameter");
+    if (c->precision < TMX_FP64 || c->precision > TMX_FP16)
+        return fail(TMX_E_INVALID, "unsupported precision %d", c->precision);
+    const long long n = (long long)c->inx * c->iny * c->nz + (long long)c->mnx * c->mny * c->nz;
+    if (n > 2000000000LL) return fail(TMX_E_INVALID, "too many nodes (%lld)", n);
+    return TMX_OK;
+}
+
+}  // namespace tmx_host
+
 extern "C" {
 
 int tmx_abi_version(void) { return TMX_ABI_VERSION; }
 
-const char* tmx_last_error(void) { return g_err.c_str(); }
+const char* tmx_last_error(void) { return last_error(); }
 
 int tmx_case_reference(tmx_case* out)
 {
@@ -458,24 +519,9 @@ int tmx_case_wlayout(int W, double u_max, double tau_f, double tau_c, double k, 
 int tmx_case_check(const tmx_case* c)
 {
     if (!c) return fail(TMX_E_INVALID, "null case");
-    if (c->inx < 3 || c->iny < 3 || c->nz < 3 || c->mnx < 3 || c->mny < 3)
-        return fail(TMX_E_INVALID, "every box size must be >= 3 (inx=%d iny=%d nz=%d mnx=%d mny=%d)", c->inx, c->iny,
-                    c->nz, c->mnx, c->mny);
-    if (c->ia < 2 || c->ia + c->mnx - 1 > c->inx - 1)
-        return fail(TMX_E_INVALID, "opening columns ia=%d..ib=%d must lie within 2..inx-1=%d", c->ia,
-                    c->ia + c->mnx - 1, c->inx - 1);
-    const double t[4] = {c->tau, c->tau_a, c->tau_b, c->tau_c};
-    for (double v : t)
-        if (!(v > 0.5) || !std::isfinite(v)) return fail(TMX_E_INVALID, "relaxation times must be finite and > 0.5");
-    if (!std::isfinite(c->rho0) || !(c->rho0 > 0) || !std::isfinite(c->rho_out) || !(c->rho_out > 0))
-        return fail(TMX_E_INVALID, "rho0 and rho_out must be finite and positive");
-    if (!std::isfinite(c->umean) || !std::isfinite(c->rateconst)) return fail(TMX_E_INVALID, "non-finite parameter");
-    if (c->precision < TMX_FP64 || c->precision > TMX_FP16)
-        return fail(TMX_E_INVALID, "unsupported precision %d", c->precision);
-    const long long n = (long long)c->inx * c->iny * c->nz + (long long)c->mnx * c->mny * c->nz;
-    if (n > 2000000000LL / 1) return fail(TMX_E_INVALID, "too many nodes (%lld)", n);
-    return TMX_OK;
+    return check_case(*c);
 }
+
 
 int tmx_case_footprint(const tmx_case* c, long long* bytes)
 {
@@ -509,33 +555,15 @@ int tmx_create(const tmx_case* c, int device, tmx_handle** out)
     h->tbytes = h->K->tbytes;
     const Geom& G = h->G;
 
-    // boundary node list, sorted by class then node index
-    std::vector<std::pair<int, int>> bl;
-    bl.reserve((size_t)boundary_count(G));
-    h->class_count.assign(tmx::K_NCLASSES, 0);
-    for (int b = 0; b < 2; b++)
-        for (int i = 1; i <= G.nx[b]; i++)
-            for (int j = 1; j <= G.ny[b]; j++)
-                for (int k = 1; k <= G.nz; k++) {
-                    if (!tmx::is_boundary(G, b, i, j, k)) continue;
-                    const int cls = classify(G, b, i, j, k);
-                    if (cls < 0) {
-                        delete h;
-                        return fail(TMX_E_INVALID, "internal: boundary node (%d,%d,%d,%d) has no class", b, i, j, k);
-                    }
-                    // faces first, then edges and corners; by class, then node
-                    bl.emplace_back((tmx::is_face_class(cls) ? 0 : 256) + cls, tmx::node_index(G, b, i, j, k));
-                    h->class_count[cls]++;
-                }
-    std::sort(bl.begin(), bl.end());
-    h->nb = (int)bl.size();
-    std::vector<int> nodes(bl.size());
-    std::vector<unsigned char> cls(bl.size());
-    for (size_t t = 0; t < bl.size(); t++) {
-        cls[t] = (unsigned char)(bl[t].first & 255);
-        nodes[t] = bl[t].second;
-        if (bl[t].first < 256) h->nface++;
+    // boundary node list, faces first, sorted by class then node index
+    std::vector<int> nodes;
+    std::vector<unsigned char> cls;
+    rc = boundary_list(G, nodes, cls, h->nface, &h->class_count);
+    if (rc) {
+        delete h;
+        return rc;
     }
+    h->nb = (int)nodes.size();
 
     auto alloc = [&](void** p, size_t n) -> cudaError_t {
         cudaError_t e = cudaMalloc(p, n);

@@ -926,18 +926,13 @@ __device__ __forceinline__ void closed_pull(const BCtx<PR>& c, int cls, int fld,
 constexpr int kBoundaryThreads = 128;
 constexpr int kBoundaryLanes = 4;
 
+// Lane fld of boundary node g (class cls); mask holds the active lanes of
+// the warp and lead the first lane of this node's group of four.
 template <class PR, bool FACES>
-__device__ __forceinline__ void boundary_node(const StepPtrs& X, const int* __restrict__ bnode,
-                                              const unsigned char* __restrict__ bcls, int nb, const Geom& G,
-                                              const Phys& P, int write_macro)
+__device__ __forceinline__ void boundary_lane(const StepPtrs& X, const Geom& G, const Phys& P, int write_macro, int g,
+                                              int cls, int fld, unsigned mask, int lead)
 {
     using T = typename PR::T;
-    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
-    const int t = gt >> 2, fld = gt & 3;
-    // the four lanes of a node share one warp; whole nodes drop out together
-    const unsigned mask = __ballot_sync(0xffffffffu, t < nb);
-    if (t >= nb) return;
-    const int lead = (threadIdx.x & 31) & ~3;
     typename PR::S* __restrict__ Pout = (typename PR::S*)X.pout;
     T* __restrict__ Rcur = (T*)X.rcur;
     double* __restrict__ Mac = X.mac;
@@ -950,9 +945,8 @@ __device__ __forceinline__ void boundary_node(const StepPtrs& X, const int* __re
     c.G = &G;
     c.P = &P;
     c.ps = G.ps;
-    c.g = bnode[t];
+    c.g = g;
     decode(G, c.g, c.b, c.i, c.j, c.k);
-    const int cls = bcls[t];
     const long long ps = G.ps;
 
     T v[19];
@@ -996,6 +990,20 @@ __device__ __forceinline__ void boundary_node(const StepPtrs& X, const int* __re
     }
 }
 
+// One launch over a node list: thread 4t + fld is lane fld of node t.
+template <class PR, bool FACES>
+__device__ __forceinline__ void boundary_node(const StepPtrs& X, const int* __restrict__ bnode,
+                                              const unsigned char* __restrict__ bcls, int nb, const Geom& G,
+                                              const Phys& P, int write_macro)
+{
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = gt >> 2, fld = gt & 3;
+    // the four lanes of a node share one warp; whole nodes drop out together
+    const unsigned mask = __ballot_sync(0xffffffffu, t < nb);
+    if (t >= nb) return;
+    boundary_lane<PR, FACES>(X, G, P, write_macro, bnode[t], bcls[t], fld, mask, (threadIdx.x & 31) & ~3);
+}
+
 // One interior node in the form's bulk scheme: one pass over the 76 values
 // for the interleaved layouts, field by field for FP64.
 template <class PR>
@@ -1029,5 +1037,43 @@ __device__ __forceinline__ void bulk_any(const StepPtrs& X, const Geom& G, const
     {                                                                                                           \
         boundary_node<PR, false>(X, bnode, bcls, nb, G, P, write_macro);                                        \
     }
+
+
+// Batched kernels for one precision policy (declared in tmx_kernels.cuh).
+#define TMX_BULK_BATCH(PR, NAME, NT)                                                                              \
+    __global__ void __launch_bounds__(NT, 512 / NT) k_bulk_batch##NT##_##NAME(                                  \
+        const MixerDesc* __restrict__ D, const int4* __restrict__ blocks, const int* __restrict__ counts,        \
+        int parity, int write_macro)                                                                            \
+    {                                                                                                           \
+        const int nblk = counts[0];                                                                             \
+        for (int b = blockIdx.x; b < nblk; b += gridDim.x) {                                                    \
+            const int4 cb = blocks[b];                                                                          \
+            const MixerDesc& d = D[cb.x];                                                                       \
+            for (int t = threadIdx.x; t < cb.z; t += NT) bulk_any<PR>(d.X[parity], d.G, d.P, write_macro, cb.y + t); \
+        }                                                                                                       \
+    }
+#define TMX_BOUNDARY_BATCH(PR, NAME, KIND, FACES, WHICH)                                                          \
+    __global__ void __launch_bounds__(kBoundaryThreads) k_##KIND##_batch_##NAME(                               \
+        const MixerDesc* __restrict__ D, const int2* __restrict__ list, const int* __restrict__ counts,         \
+        int parity, int write_macro)                                                                            \
+    {                                                                                                           \
+        const int n = counts[WHICH];                                                                            \
+        for (int base = blockIdx.x * blockDim.x; base < 4 * n; base += gridDim.x * blockDim.x) {                \
+            const int t = (base + threadIdx.x) >> 2, fld = threadIdx.x & 3;                                     \
+            const unsigned mask = __ballot_sync(0xffffffffu, t < n);                                            \
+            if (t < n) {                                                                                        \
+                const int2 e = list[t];                                                                         \
+                const MixerDesc& d = D[e.y >> 8];                                                               \
+                boundary_lane<PR, FACES>(d.X[parity], d.G, d.P, write_macro, e.x, e.y & 255, fld, mask,         \
+                                         (threadIdx.x & 31) & ~3);                                              \
+            }                                                                                                   \
+        }                                                                                                       \
+    }
+#define TMX_DEFINE_BATCH_KERNELS(PR, NAME)        \
+    TMX_BULK_BATCH(PR, NAME, 128)                 \
+    TMX_BULK_BATCH(PR, NAME, 256)                 \
+    TMX_BULK_BATCH(PR, NAME, 512)                 \
+    TMX_BOUNDARY_BATCH(PR, NAME, bfaces, true, 1) \
+    TMX_BOUNDARY_BATCH(PR, NAME, bedges, false, 2)
 
 }  // namespace tmx

@@ -9,6 +9,7 @@
 namespace tmx {
 
 TMX_DEFINE_STEP_KERNELS(F64, f64)
+TMX_DEFINE_BATCH_KERNELS(F64, f64)
 
 // ---------------------------------------------------------------------------
 // mixing quality (Tmixer.cpp:10161-10409): per row, per species, the sums of
@@ -16,16 +17,15 @@ TMX_DEFINE_STEP_KERNELS(F64, f64)
 // thread block per row; thread s handles species s.  Rows: mixing 1..mny,
 // then inlet 1..iny over x = ia..ib.
 // ---------------------------------------------------------------------------
-__global__ void k_mixing_rows(const double* __restrict__ Mac, Geom G, double* __restrict__ stats)
+__device__ __forceinline__ void row_stats(const double* __restrict__ Mac, const Geom& G, int row, int s, double& avg,
+                                          double& var, double& mx)
 {
-    const int row = blockIdx.x;
-    const int s = threadIdx.x;
-    if (s >= 3) return;
     const int b = row < G.mny ? 1 : 0;
     const int j = b == 1 ? row + 1 : row - G.mny + 1;
     const int i0 = b == 1 ? 1 : G.ia, i1 = b == 1 ? G.mnx : G.ib;
     const double* cfield = Mac + (long long)(4 + s) * G.ps;
-    double sumx = 0.0, mx = __longlong_as_double(0xfff0000000000000ULL);  // -inf
+    double sumx = 0.0;
+    mx = __longlong_as_double(0xfff0000000000000ULL);  // -inf
     for (int i = i0; i <= i1; i++) {
         double sumz = 0.0;
         for (int k = 1; k <= G.nz; k++) {
@@ -35,7 +35,7 @@ __global__ void k_mixing_rows(const double* __restrict__ Mac, Geom G, double* __
         }
         sumx += sumz;
     }
-    const double avg = (sumx / (1.0 * G.nz * G.mnx));
+    avg = (sumx / (1.0 * G.nz * G.mnx));
     sumx = 0.0;
     for (int i = i0; i <= i1; i++) {
         double sumz = 0.0;
@@ -45,10 +45,42 @@ __global__ void k_mixing_rows(const double* __restrict__ Mac, Geom G, double* __
         }
         sumx += sumz;
     }
-    const double var = (1.0 / (1.0 * G.nz * G.mnx)) * sumx;
+    var = (1.0 / (1.0 * G.nz * G.mnx)) * sumx;
+}
+
+__global__ void k_mixing_rows(const double* __restrict__ Mac, Geom G, double* __restrict__ stats)
+{
+    const int row = blockIdx.x;
+    const int s = threadIdx.x;
+    if (s >= 3) return;
+    double avg, var, mx;
+    row_stats(Mac, G, row, s, avg, var, mx);
     stats[row * 9 + s] = avg;
     stats[row * 9 + 3 + s] = var;
     stats[row * 9 + 6 + s] = mx;
+}
+
+// Outlet row (mixing row 1, the first row of the reference's order) of batch
+// mixers: its running maximum is max(0, the row's maximum).  One block per
+// entry, thread s handles species s.
+__global__ void k_outlet_im_batch(const MixerDesc* __restrict__ D, const int* __restrict__ slots, int n,
+                                  double* __restrict__ out)
+{
+    const int e = blockIdx.x, s = threadIdx.x;
+    __shared__ double avgs[3];
+    if (e >= n) return;
+    const MixerDesc& d = D[slots[e]];
+    double avg = 0.0, var = 0.0, m = 0.0;
+    if (s < 3) {
+        row_stats(d.X[0].mac, d.G, 0, s, avg, var, m);
+        avgs[s] = avg;
+    }
+    __syncthreads();
+    if (s >= 3) return;
+    double mx = 0.0;
+    if (mx < m) mx = m;
+    const bool ok = avgs[0] > 0 && avgs[1] > 0 && avgs[2] > 0;
+    out[3 * e + s] = ok ? 1.0 - sqrt(var / (avg * (mx - avg))) : 0.0;
 }
 
 // ---------------------------------------------------------------------------

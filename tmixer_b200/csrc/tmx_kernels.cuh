@@ -37,6 +37,43 @@ TMX_DECLARE_STEP_KERNELS(f64)
 TMX_DECLARE_STEP_KERNELS(f32)
 TMX_DECLARE_STEP_KERNELS(f16)
 
+// One mixer of a batch: its buffers for either parity of the batch's step
+// counter, its geometry and its physics constants (device memory, read by
+// the batched kernels).
+struct MixerDesc {
+    StepPtrs X[2];
+    Geom G;
+    Phys P;
+};
+
+// Batched step kernels: one launch covers every mixer of a batch.
+//   bulk    a persistent grid walks a list of cell blocks {mixer, first
+//           node, node count, 0}; NT threads per block (128, 256 or 512).
+//   faces / edges   boundary-node lists of {node, mixer * 256 + class},
+//           four threads per node, persistent grid.
+// counts[0..2] = number of cell blocks, face nodes, edge nodes (device
+// memory, so that captured graphs stay valid when the batch changes).
+#define TMX_DECLARE_BATCH_KERNELS(NAME)                                                                           \
+    __global__ void k_bulk_batch128_##NAME(const MixerDesc* D, const int4* blocks, const int* counts, int parity, \
+                                           int write_macro);                                                      \
+    __global__ void k_bulk_batch256_##NAME(const MixerDesc* D, const int4* blocks, const int* counts, int parity, \
+                                           int write_macro);                                                      \
+    __global__ void k_bulk_batch512_##NAME(const MixerDesc* D, const int4* blocks, const int* counts, int parity, \
+                                           int write_macro);                                                      \
+    __global__ void k_bfaces_batch_##NAME(const MixerDesc* D, const int2* list, const int* counts, int parity,    \
+                                          int write_macro);                                                       \
+    __global__ void k_bedges_batch_##NAME(const MixerDesc* D, const int2* list, const int* counts, int parity,    \
+                                          int write_macro);
+
+TMX_DECLARE_BATCH_KERNELS(f64)
+TMX_DECLARE_BATCH_KERNELS(f32)
+TMX_DECLARE_BATCH_KERNELS(f16)
+
+// Outlet mixing quality of batch mixers: for entry e, mixer slots[e], the
+// I_A, I_B, I_C of mixing row 1 (the first row of tmx_mixing) into
+// out[3e..3e+2], with the arithmetic of k_mixing_rows and its finish.
+__global__ void k_outlet_im_batch(const MixerDesc* D, const int* slots, int n, double* out);
+
 __global__ void k_mixing_rows(const double* __restrict__ Mac, Geom G, double* __restrict__ stats);
 __global__ void k_sums(const double* __restrict__ Mac, Geom G, double* __restrict__ partial);
 
