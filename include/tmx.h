@@ -260,6 +260,64 @@ int tmx_batch_time_steps(tmx_batch *b, int nsteps, double *ms);
 /* Free the batch, its arena and its mixers. */
 void tmx_batch_destroy(tmx_batch *b);
 
+/* ------------------------------------------------------------------------
+ * Served form: a request loop over a batch (continuous batching).  Requests
+ * arrive over time; each is admitted as soon as it has arrived, every
+ * earlier request has been admitted and its footprint fits in the batch's
+ * free arena; admitted mixers step together; every check_every steps the
+ * outlet mixing index of each is read and a mixer is retired once, over its
+ * last window steps, every species' index was non-zero (the species have
+ * reached the outlet) and moved by less than tol, or after max_steps; a
+ * retired mixer's range is back-filled by the next request.  No
+ * counterpart in the reference.
+ * ------------------------------------------------------------------------ */
+typedef struct tmx_request {
+    tmx_case c;
+    double arrival; /* seconds after the start of the loop */
+    int max_steps;  /* retire after this many steps at most */
+    int window;     /* convergence window (steps), a multiple of check_every */
+    double tol;     /* convergence tolerance of the outlet mixing index */
+} tmx_request;
+
+typedef struct tmx_served {
+    int status;         /* 0 converged, 1 stopped at max_steps, TMX_E_NOMEM larger than the whole budget */
+    int slot;           /* batch slot it ran in */
+    long long steps;    /* steps taken */
+    double admitted;    /* seconds after the start */
+    double finished;    /* seconds after the start (time to solution = finished - arrival) */
+    double outlet_im[3]; /* outlet I_A, I_B, I_C when retired */
+} tmx_served;
+
+typedef struct tmx_serve_opts {
+    int check_every; /* steps between convergence checks */
+    int max_active;  /* at most this many mixers at once (0: no limit but the budget) */
+} tmx_serve_opts;
+
+/* summary[0] makespan (s, from the start to the last retirement), [1] lattice
+ * updates (fluid nodes x steps, all requests), [2] aggregate MLUPS, [3] p50
+ * and [4] p99 time to solution (s), [5] most mixers at once, [6] time-weighted
+ * mean mixers at once, [7] convergence checks made. */
+int tmx_serve(tmx_batch *b, const tmx_request *reqs, int n, const tmx_serve_opts *opts, tmx_served *out,
+              double summary[8]);
+
+/* The same loop over an engine given as callbacks (for testing the scheduler
+ * without a GPU, or driving another engine).  Each callback returns 0 or a
+ * TMX_E_* code; add returns TMX_E_NOMEM when the mixer does not fit now. */
+typedef struct tmx_serve_ops {
+    void *ctx;
+    int (*footprint)(void *ctx, const tmx_case *c, long long *bytes);
+    long long (*capacity)(void *ctx);
+    int (*add)(void *ctx, const tmx_case *c, int *slot);
+    int (*remove)(void *ctx, int slot);
+    int (*step)(void *ctx, int nsteps);
+    int (*outlet_im)(void *ctx, const int *slots, int n, double *im);
+    double (*now)(void *ctx);
+    void (*wait_until)(void *ctx, double t);
+} tmx_serve_ops;
+
+int tmx_serve_with(const tmx_serve_ops *ops, const tmx_request *reqs, int n, const tmx_serve_opts *opts,
+                   tmx_served *out, double summary[8]);
+
 #ifdef __cplusplus
 }
 #endif

@@ -52,6 +52,36 @@ class _CCase(ctypes.Structure):
                 ("umean", ctypes.c_double), ("precision", ctypes.c_int)]
 
 
+class _CRequest(ctypes.Structure):
+    _fields_ = [("c", _CCase), ("arrival", ctypes.c_double), ("max_steps", ctypes.c_int), ("window", ctypes.c_int),
+                ("tol", ctypes.c_double)]
+
+
+class _CServed(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("slot", ctypes.c_int), ("steps", ctypes.c_longlong),
+                ("admitted", ctypes.c_double), ("finished", ctypes.c_double), ("outlet_im", ctypes.c_double * 3)]
+
+
+class _CServeOpts(ctypes.Structure):
+    _fields_ = [("check_every", ctypes.c_int), ("max_active", ctypes.c_int)]
+
+
+_FOOTPRINT = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(_CCase), ctypes.POINTER(ctypes.c_longlong))
+_CAPACITY = ctypes.CFUNCTYPE(ctypes.c_longlong, ctypes.c_void_p)
+_ADD = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(_CCase), ctypes.POINTER(ctypes.c_int))
+_REMOVE = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int)
+_STEP = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int)
+_OUTLET = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.c_int,
+                           ctypes.POINTER(ctypes.c_double))
+_NOW = ctypes.CFUNCTYPE(ctypes.c_double, ctypes.c_void_p)
+_WAIT = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_double)
+
+
+class _CServeOps(ctypes.Structure):
+    _fields_ = [("ctx", ctypes.c_void_p), ("footprint", _FOOTPRINT), ("capacity", _CAPACITY), ("add", _ADD),
+                ("remove", _REMOVE), ("step", _STEP), ("outlet_im", _OUTLET), ("now", _NOW), ("wait_until", _WAIT)]
+
+
 _lib = None
 
 
@@ -106,6 +136,8 @@ def lib() -> ctypes.CDLL:
     L.tmx_batch_time_steps.argtypes = [vp, ip, P(dp)]
     L.tmx_batch_destroy.argtypes = [vp]
     L.tmx_batch_destroy.restype = None
+    L.tmx_serve.argtypes = [vp, P(_CRequest), ip, P(_CServeOpts), P(_CServed), P(dp)]
+    L.tmx_serve_with.argtypes = [P(_CServeOps), P(_CRequest), ip, P(_CServeOpts), P(_CServed), P(dp)]
     if L.tmx_abi_version() != ABI_VERSION:
         raise RuntimeError("libtmx.so ABI %d, expected %d" % (L.tmx_abi_version(), ABI_VERSION))
     _lib = L
@@ -413,5 +445,103 @@ class Batch:
             pass
 
 
-__all__ = ["CaseSpec", "Solver", "Batch", "TmxError", "FIELDS", "TMX_FP64", "TMX_FP32", "TMX_FP16", "PRECISIONS",
+@dataclasses.dataclass
+class Request:
+    """One solve of the served form: a case, its arrival time (seconds after
+    the loop starts) and its stopping rule."""
+    spec: CaseSpec
+    arrival: float = 0.0
+    max_steps: int = 50000
+    window: int = 500
+    tol: float = 1e-6
+
+    def to_c(self) -> _CRequest:
+        return _CRequest(self.spec.to_c(), float(self.arrival), int(self.max_steps), int(self.window),
+                         float(self.tol))
+
+
+SERVE_STATUS = {0: "converged", 1: "max_steps", -2: "too large for the budget"}
+
+
+def _serve_out(reqs, res, summ):
+    results = [dict(status=SERVE_STATUS.get(r.status, r.status), slot=r.slot, steps=r.steps, arrival=q.arrival,
+                    admitted=r.admitted, finished=r.finished, time_to_solution=r.finished - q.arrival,
+                    outlet_im=list(r.outlet_im)) for q, r in zip(reqs, res)]
+    summary = dict(makespan_s=summ[0], lattice_updates=summ[1], mlups=summ[2], p50_s=summ[3], p99_s=summ[4],
+                   max_active=int(summ[5]), mean_active=summ[6], checks=int(summ[7]))
+    return results, summary
+
+
+def serve(batch: "Batch", requests, check_every: int = 100, max_active: int = 0):
+    """Run the request loop (tmx_serve) over a batch; returns (per-request
+    results, summary with makespan, aggregate MLUPS and p50/p99 time to
+    solution)."""
+    reqs = list(requests)
+    arr = (_CRequest * max(1, len(reqs)))(*[q.to_c() for q in reqs])
+    res = (_CServed * max(1, len(reqs)))()
+    opts = _CServeOpts(int(check_every), int(max_active))
+    summ = (ctypes.c_double * 8)()
+    _check(lib().tmx_serve(batch._b, arr, len(reqs), ctypes.byref(opts), res, summ))
+    return _serve_out(reqs, res[:len(reqs)], summ)
+
+
+def serve_with(engine, requests, check_every: int = 100, max_active: int = 0):
+    """Run the same request loop (tmx_serve_with) over a Python engine object
+    with methods footprint(spec), capacity(), add(spec) -> slot or None when it
+    does not fit now, remove(slot), step(n), outlet_im(slots) -> (n, 3),
+    now(), wait_until(t).  For tests of the scheduler without a GPU."""
+    reqs = list(requests)
+    errors = []
+
+    def guard(fn, fail=-3):
+        def w(*a):
+            try:
+                return fn(*a)
+            except Exception as e:  # pragma: no cover - surfaced below
+                errors.append(e)
+                return fail
+        return w
+
+    def fp(_, c, out):
+        out[0] = int(engine.footprint(CaseSpec.from_c(c.contents)))
+        return 0
+
+    def add(_, c, slot):
+        s = engine.add(CaseSpec.from_c(c.contents))
+        if s is None:
+            return -2
+        slot[0] = int(s)
+        return 0
+
+    def rem(_, slot):
+        engine.remove(int(slot))
+        return 0
+
+    def step(_, n):
+        engine.step(int(n))
+        return 0
+
+    def im(_, slots, n, out):
+        v = np.asarray(engine.outlet_im([slots[i] for i in range(n)]), dtype=np.float64).reshape(n, 3)
+        for i in range(n):
+            for s in range(3):
+                out[3 * i + s] = float(v[i, s])
+        return 0
+
+    cbs = [_FOOTPRINT(guard(fp)), _CAPACITY(guard(lambda _: int(engine.capacity()), 0)), _ADD(guard(add)),
+           _REMOVE(guard(rem)), _STEP(guard(step)), _OUTLET(guard(im)), _NOW(guard(lambda _: float(engine.now()), 0.0)),
+           _WAIT(guard(lambda _, t: engine.wait_until(float(t)), None))]
+    ops = _CServeOps(None, *cbs)
+    arr = (_CRequest * max(1, len(reqs)))(*[q.to_c() for q in reqs])
+    res = (_CServed * max(1, len(reqs)))()
+    opts = _CServeOpts(int(check_every), int(max_active))
+    summ = (ctypes.c_double * 8)()
+    rc = lib().tmx_serve_with(ctypes.byref(ops), arr, len(reqs), ctypes.byref(opts), res, summ)
+    if errors:
+        raise errors[0]
+    _check(rc)
+    return _serve_out(reqs, res[:len(reqs)], summ)
+
+
+__all__ = ["CaseSpec", "Solver", "Batch", "Request", "serve", "serve_with", "TmxError", "FIELDS", "TMX_FP64", "TMX_FP32", "TMX_FP16", "PRECISIONS",
            "reference_case", "w_layout", "lib"]

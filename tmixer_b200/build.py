@@ -22,6 +22,9 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC"]
 # operation separately rounded; the reduced-precision kernels may fuse
 SOURCES = {"tmx_kernels.cu": ["--fmad=false"], "tmx_api.cu": ["--fmad=false"], "tmx_kernels_lp.cu": ["--fmad=true"],
            "tmx_batch.cu": ["--fmad=false"]}
+# host-only C++ sources of the library (no device code)
+CXX_SOURCES = {"tmx_serve.cpp": []}
+CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall"]
 OBJDIR = os.path.join(PKG, "_build")
 
 
@@ -50,6 +53,15 @@ def build(force: bool = False, verbose: bool = False) -> str:
         objs.append(obj)
         if force or _stale(obj, [path] + headers):
             cmd = [_nvcc()] + NVCC_FLAGS + flags + ARCH + ["-c", "-o", obj, path]
+            if verbose:
+                print(" ".join(cmd), file=sys.stderr)
+            jobs.append((cmd, subprocess.Popen(cmd)))
+    for src, flags in CXX_SOURCES.items():
+        path = os.path.join(CSRC, src)
+        obj = os.path.join(OBJDIR, src + ".o")
+        objs.append(obj)
+        if force or _stale(obj, [path] + headers):
+            cmd = ["g++"] + CXX_FLAGS + flags + ["-c", "-o", obj, path]
             if verbose:
                 print(" ".join(cmd), file=sys.stderr)
             jobs.append((cmd, subprocess.Popen(cmd)))
