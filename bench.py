@@ -482,7 +482,7 @@ def main(argv=None) -> int:
     ap.add_argument("--no-served", action="store_true", help="skip the served form")
     ap.add_argument("--batched-mixers", type=int, default=64)
     ap.add_argument("--batched-steps", type=int, default=5000)
-    ap.add_argument("--served-requests", type=int, default=16)
+    ap.add_argument("--served-requests", type=int, default=8)
     ap.add_argument("--served-max-steps", type=int, default=50000)
 
     args = ap.parse_args(argv)

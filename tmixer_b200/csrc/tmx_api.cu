@@ -705,11 +705,11 @@ int tmx_populations(tmx_handle* h, int box, int fld, double* host_out)
     // the writing node's moments exactly as the kernels do (tmx_engine.cuh)
     std::vector<double> wide(n);
     std::vector<unsigned char> raw(4 * n * h->sbytes);
-    std::vector<float> mf(4 * n), ms(4 * n);
+    // moment records {(rho, ux, uy, uz), (cA, cB, cC, t)}, 8 floats per node
+    std::vector<float> mr(8 * n);
     if (h->K->moments) {
         const float4* m = h->mom[h->cur];
-        TMX_CK(cudaMemcpy(mf.data(), m + G.base[box], n * sizeof(float4), cudaMemcpyDeviceToHost));
-        TMX_CK(cudaMemcpy(ms.data(), m + G.ps + G.base[box], n * sizeof(float4), cudaMemcpyDeviceToHost));
+        TMX_CK(cudaMemcpy(mr.data(), m + 2 * (size_t)G.base[box], n * 2 * sizeof(float4), cudaMemcpyDeviceToHost));
     }
     for (int q = 0; q < 19; q++) {
         // interleaved layout: the four fields of (q, node) side by side
@@ -725,8 +725,9 @@ int tmx_populations(tmx_handle* h, int box, int fld, double* host_out)
             } else {
                 unsigned short hb;
                 std::memcpy(&hb, &raw[e], 2);
-                const float r = fld == 0 ? mf[4 * t] : ms[4 * t + fld - 1];
-                v = half_bits_to_float(hb) + (r * poly_q_host(q, mf[4 * t + 1], mf[4 * t + 2], mf[4 * t + 3])) * w;
+                const float* rec = &mr[8 * t];
+                const float r = fld == 0 ? rec[0] : rec[3 + fld];
+                v = half_bits_to_float(hb) + r * (poly_q_host(q, rec[1], rec[2], rec[3]) * w);
             }
             wide[t] = v;
         }

@@ -84,20 +84,24 @@ __host__ __device__ inline void decode(const Geom& G, int g, int& b, int& i, int
 // mny takes 4,9,10,16,17 from inlet row 1, :9230-9237).  -1 for a source
 // outside both boxes (a ghost node; every such value is replaced by a
 // boundary closure).
-__host__ __device__ inline int pull_src(const Geom& G, int b, int i, int j, int k, int q)
+__host__ __device__ inline int pull_src_e(const Geom& G, int b, int i, int j, int k, int ex, int ey, int ez)
 {
-    int si = i - EX(q), sj = j - EY(q), sk = k - EZ(q), sb = b;
-    if (b == 0 && j == 1 && EY(q) == 1 && i >= G.ia && i <= G.ib) {
+    int si = i - ex, sj = j - ey, sk = k - ez, sb = b;
+    if (b == 0 && j == 1 && ey == 1 && i >= G.ia && i <= G.ib) {
         sb = 1;
-        si = i - G.ia + 1 - EX(q);
+        si = i - G.ia + 1 - ex;
         sj = G.mny;
-    } else if (b == 1 && j == G.mny && EY(q) == -1) {
+    } else if (b == 1 && j == G.mny && ey == -1) {
         sb = 0;
-        si = i + G.ia - 1 - EX(q);
+        si = i + G.ia - 1 - ex;
         sj = 1;
     }
     if (si < 1 || si > box_nx(G, sb) || sj < 1 || sj > box_ny(G, sb) || sk < 1 || sk > G.nz) return -1;
     return node_index(G, sb, si, sj, sk);
+}
+__host__ __device__ inline int pull_src(const Geom& G, int b, int i, int j, int k, int q)
+{
+    return pull_src_e(G, b, i, j, k, EX(q), EY(q), EZ(q));
 }
 
 // x / d for the constants d = 3, 18, 36, correctly rounded, without a
@@ -138,12 +142,17 @@ __device__ __forceinline__ double wq(int q) { return q == 0 ? 1.0 / 3.0 : (q <= 
 // result (which the equilibrium polynomial absorbs), so only the sum of the
 // two non-zero terms rounds; q is a compile-time constant after unrolling.
 template <class T>
+__device__ __forceinline__ T e_dot_u_e(int ex, int ey, int ez, T ux, T uy, T uz)
+{
+    const T a = ex > 0 ? ux : -ux, b = ey > 0 ? uy : -uy, c = ez > 0 ? uz : -uz;
+    if (ex != 0) return ey != 0 ? a + b : (ez != 0 ? a + c : a);
+    if (ey != 0) return ez != 0 ? b + c : b;
+    return ez != 0 ? c : T(0);
+}
+template <class T>
 __device__ __forceinline__ T e_dot_u(int q, T ux, T uy, T uz)
 {
-    const T a = EX(q) > 0 ? ux : -ux, b = EY(q) > 0 ? uy : -uy, c = EZ(q) > 0 ? uz : -uz;
-    if (EX(q) != 0) return EY(q) != 0 ? a + b : (EZ(q) != 0 ? a + c : a);
-    if (EY(q) != 0) return EZ(q) != 0 ? b + c : b;
-    return EZ(q) != 0 ? c : T(0);
+    return e_dot_u_e(EX(q), EY(q), EZ(q), ux, uy, uz);
 }
 
 // Equilibrium polynomial shared by the four fields (they use the flow

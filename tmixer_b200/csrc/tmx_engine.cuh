@@ -48,11 +48,16 @@ __device__ __forceinline__ float u2_term(float ux, float uy, float uz)
 {
     return __fmul_rn(1.5f, __fadd_rn(__fadd_rn(__fmul_rn(ux, ux), __fmul_rn(uy, uy)), __fmul_rn(uz, uz)));
 }
+// direction given by its lattice vector (ex, ey, ez), possibly run-time values
+__device__ __forceinline__ float poly_e_rn_t(int ex, int ey, int ez, float ux, float uy, float uz, float t)
+{
+    if ((ex | ey | ez) == 0) return __fsub_rn(1.0f, t);
+    const float eu = e_dot_u_e(ex, ey, ez, ux, uy, uz);
+    return __fadd_rn(__fsub_rn(__fadd_rn(1.0f, __fmul_rn(3.0f, eu)), t), __fmul_rn(__fmul_rn(4.5f, eu), eu));
+}
 __device__ __forceinline__ float poly_q_rn_t(int q, float ux, float uy, float uz, float t)
 {
-    if (q == 0) return __fsub_rn(1.0f, t);
-    const float eu = e_dot_u(q, ux, uy, uz);
-    return __fadd_rn(__fsub_rn(__fadd_rn(1.0f, __fmul_rn(3.0f, eu)), t), __fmul_rn(__fmul_rn(4.5f, eu), eu));
+    return poly_e_rn_t(EX(q), EY(q), EZ(q), ux, uy, uz, t);
 }
 __device__ __forceinline__ float poly_q_rn(int q, float ux, float uy, float uz)
 {
@@ -108,9 +113,30 @@ struct F32 {
     {
         *(float4*)p = make_float4(v[0], v[1], v[2], v[3]);
     }
-    __device__ static void poly(T ux, T uy, T uz, T (&p)[19]) { eq_poly(ux, uy, uz, p); }
+    // poly holds w_q * poly_q, so that an equilibrium value is one multiply
+    __device__ static void poly(T ux, T uy, T uz, T (&p)[19])
+    {
+        eq_poly(ux, uy, uz, p);
+#pragma unroll
+        for (int q = 0; q < 19; q++) p[q] = p[q] * (float)wq(q);
+    }
     __device__ static bool tiny(T) { return false; }
-    __device__ static T feq(T r, T polyq, int q, bool) { return r * polyq * (float)wq(q); }
+    __device__ static T feq(T r, T pw, int, bool) { return r * pw; }
+    // w * poly of one direction given by (ex, ey, ez) and weight w
+    __device__ static T pw_dir(int ex, int ey, int ez, T w, T ux, T uy, T uz)
+    {
+        const T u2 = ux * ux + uy * uy + uz * uz;
+        const T t = T(3) * u2 / T(2);
+        if ((ex | ey | ez) == 0) return (T(1) - t) * w;
+        const T eu = e_dot_u_e(ex, ey, ez, ux, uy, uz);
+        return (T(1) + T(3) * eu - t + T(9) * eu * eu / T(2)) * w;
+    }
+    // the four fields pulled from source s along (ex, ey, ez) of direction q
+    __device__ static void decode4(const S* __restrict__ Pin, const float4* __restrict__, long long ps, int q, int,
+                                   int, int, T, int s, T (&v)[4])
+    {
+        load4(Pin + off(0, q, ps, s), v);
+    }
     __device__ static T decode(const S* p, int, int, const float4*, long long, int) { return __ldg(p); }
     __device__ static void encode(S* p, T v, T) { *p = v; }
     __device__ static T raw(const S* p) { return __ldg(p); }
@@ -118,7 +144,8 @@ struct F32 {
 
 // FP32 arithmetic; populations stored in FP16 as their non-equilibrium part
 // n_q = f_q - feq_q(rho, u) of the node that wrote them, next to that node's
-// FP32 moments M = {(rho, ux, uy, uz), (cA, cB, cC, 1.5|u|^2)} (float4[2*ps]).  A
+// FP32 moments M = {(rho, ux, uy, uz), (cA, cB, cC, 1.5|u|^2)}, one 32-byte
+// record per node (float4 M[2g], M[2g+1]).  A
 // reader adds back feq_q of the writer's moments.  The stored quantity is of
 // the order of the gradients, so FP16 keeps about FP32 accuracy of f.
 struct F16 {
@@ -149,23 +176,40 @@ struct F16 {
         x.y = *(const unsigned*)&hi;
         *(uint2*)p = x;
     }
+    // poly holds w_q * poly_q (rounded as below), so that an equilibrium
+    // value is one multiply
     __device__ static void poly(T ux, T uy, T uz, T (&p)[19])
     {
 #pragma unroll
-        for (int q = 0; q < 19; q++) p[q] = poly_q_rn(q, ux, uy, uz);
+        for (int q = 0; q < 19; q++) p[q] = __fmul_rn(poly_q_rn(q, ux, uy, uz), (float)wq(q));
     }
     __device__ static bool tiny(T) { return false; }
-    __device__ static T feq(T r, T polyq, int q, bool) { return __fmul_rn(__fmul_rn(r, polyq), (float)wq(q)); }
-    __device__ static T decode(const S* p, int fld, int q, const float4* M, long long ps, int src)
+    __device__ static T feq(T r, T pw, int, bool) { return __fmul_rn(r, pw); }
+    // w_q * poly_q of a writer from its moment record {(rho, u), (c, t)}
+    __device__ static T src_pw(int q, const float4& mf, const float4& ms)
     {
-        const float4 mf = __ldg(M + src);
-        float r = mf.x;
-        if (fld > 0) {
-            const float4 ms = __ldg(M + ps + src);
-            r = fld == 1 ? ms.x : (fld == 2 ? ms.y : ms.z);
-        }
-        const float t = __ldg(&M[ps + src].w);
-        return __half2float(__ldg(p)) + feq(r, poly_q_rn_t(q, mf.y, mf.z, mf.w, t), q, false);
+        return __fmul_rn(poly_q_rn_t(q, mf.y, mf.z, mf.w, ms.w), (float)wq(q));
+    }
+    __device__ static T pw_dir(int ex, int ey, int ez, T w, T ux, T uy, T uz)
+    {
+        return __fmul_rn(poly_e_rn_t(ex, ey, ez, ux, uy, uz, u2_term(ux, uy, uz)), w);
+    }
+    __device__ static void decode4(const S* __restrict__ Pin, const float4* __restrict__ M, long long ps, int q,
+                                   int ex, int ey, int ez, T w, int s, T (&v)[4])
+    {
+        load4(Pin + off(0, q, ps, s), v);
+        const float4 mf = __ldg(M + 2 * (long long)s), ms = __ldg(M + 2 * (long long)s + 1);
+        const float pw = __fmul_rn(poly_e_rn_t(ex, ey, ez, mf.y, mf.z, mf.w, ms.w), w);
+        v[0] = v[0] + feq(mf.x, pw, q, false);
+        v[1] = v[1] + feq(ms.x, pw, q, false);
+        v[2] = v[2] + feq(ms.y, pw, q, false);
+        v[3] = v[3] + feq(ms.z, pw, q, false);
+    }
+    __device__ static T decode(const S* p, int fld, int q, const float4* M, long long, int src)
+    {
+        const float4 mf = __ldg(M + 2 * (long long)src), ms = __ldg(M + 2 * (long long)src + 1);
+        const float r = fld == 0 ? mf.x : (fld == 1 ? ms.x : (fld == 2 ? ms.y : ms.z));
+        return __half2float(__ldg(p)) + feq(r, src_pw(q, mf, ms), q, false);
     }
     __device__ static void encode(S* p, T v, T feq) { *p = __float2half_rn(v - feq); }
     __device__ static T raw(const S* p) { return __half2float(__ldg(p)); }
@@ -263,9 +307,14 @@ __device__ __forceinline__ void init_node(const StepPtrs& X, const Geom& G, cons
     T f[19], z[19];
 #pragma unroll
     for (int q = 0; q < 19; q++) {
-        const T d = q == 0 ? T(3) : (q <= 6 ? T(18) : T(36));
-        f[q] = (rho0 * poly[q]) / d;
-        z[q] = (T(0) * poly[q]) / d;
+        if constexpr (PR::kOnePass) {  // poly holds w_q * poly_q
+            f[q] = PR::feq(rho0, poly[q], q, false);
+            z[q] = T(0);
+        } else {
+            const T d = q == 0 ? T(3) : (q <= 6 ? T(18) : T(36));
+            f[q] = (rho0 * poly[q]) / d;
+            z[q] = (T(0) * poly[q]) / d;
+        }
     }
     const T rt = T(P.rateconst) * T(0) * T(0);
     collide_store<PR>(Pout, ps, g, 0, f, rho0, poly, P, rt);
@@ -280,8 +329,8 @@ __device__ __forceinline__ void init_node(const StepPtrs& X, const Geom& G, cons
 #pragma unroll
     for (int m = 1; m < 7; m++) Mac[m * ps + g] = 0.0;
     if (PR::kMoments) {
-        X.mcur[g] = make_float4((float)rho0, 0.f, 0.f, 0.f);
-        X.mcur[ps + g] = make_float4(0.f, 0.f, 0.f, 0.f);
+        X.mcur[2 * (long long)g] = make_float4((float)rho0, 0.f, 0.f, 0.f);
+        X.mcur[2 * (long long)g + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
 }
 
@@ -376,8 +425,9 @@ __device__ __forceinline__ void bulk_node(const StepPtrs& X, const Geom& G, cons
         Rcur[3 * ps + g] = cc;
     }
     if (PR::kMoments) {
-        X.mcur[g] = make_float4((float)rho, (float)ux, (float)uy, (float)uz);
-        X.mcur[ps + g] = make_float4((float)ca, (float)cb, (float)cc, u2_term((float)ux, (float)uy, (float)uz));
+        X.mcur[2 * (long long)g] = make_float4((float)rho, (float)ux, (float)uy, (float)uz);
+        X.mcur[2 * (long long)g + 1] =
+            make_float4((float)ca, (float)cb, (float)cc, u2_term((float)ux, (float)uy, (float)uz));
     }
     if (write_macro) {
         double* Mac = X.mac;
@@ -416,9 +466,9 @@ __device__ __forceinline__ void bulk_node_lp(const StepPtrs& X, const Geom& G, c
         T raw[4];
         PR::load4(Pin + PR::off(0, q, ps, s), raw);
         T e0 = T(0), e1 = T(0), e2 = T(0), e3 = T(0);
-        if (PR::kMoments) {
-            const float4 mf = __ldg(M + s), ms = __ldg(M + ps + s);
-            const float pq = poly_q_rn_t(q, mf.y, mf.z, mf.w, ms.w);
+        if constexpr (PR::kMoments) {
+            const float4 mf = __ldg(M + 2 * (long long)s), ms = __ldg(M + 2 * (long long)s + 1);
+            const float pq = PR::src_pw(q, mf, ms);
             e0 = PR::feq(mf.x, pq, q, false);
             e1 = PR::feq(ms.x, pq, q, false);
             e2 = PR::feq(ms.y, pq, q, false);
@@ -446,8 +496,9 @@ __device__ __forceinline__ void bulk_node_lp(const StepPtrs& X, const Geom& G, c
         Rcur[3 * ps + g] = cc;
     }
     if (PR::kMoments) {
-        X.mcur[g] = make_float4((float)rho, (float)ux, (float)uy, (float)uz);
-        X.mcur[ps + g] = make_float4((float)ca, (float)cb, (float)cc, u2_term((float)ux, (float)uy, (float)uz));
+        X.mcur[2 * (long long)g] = make_float4((float)rho, (float)ux, (float)uy, (float)uz);
+        X.mcur[2 * (long long)g + 1] =
+            make_float4((float)ca, (float)cb, (float)cc, u2_term((float)ux, (float)uy, (float)uz));
     }
     if (write_macro) {
         double* Mac = X.mac;
@@ -888,21 +939,29 @@ __device__ __forceinline__ void closure_edge(const BCtx<PR>& c, int cls, int fld
 // The post-closure populations of field fld of the boundary node in c.  A
 // species on a wall face is a zero-gradient copy of an interior node's pulled
 // populations (Tmixer.cpp:2766-4237), so it pulls that node directly.
+// The interior neighbour whose pulled species populations a face node copies
+// (zero-gradient closure), or (0, 0, 0) for a face without that closure.
+__device__ __forceinline__ void face_copy_offset(int cls, int& di, int& dj, int& dk)
+{
+    di = dj = dk = 0;
+    switch (cls) {
+    case K_FACE_YT: dj = -1; break;
+    case K_FACE_Y1:
+    case K_OUTLET: dj = 1; break;
+    case K_FACE_MX1: di = 1; break;
+    case K_FACE_MXT: di = -1; break;
+    case K_FACE_ZT: dk = -1; break;
+    case K_FACE_Z1: dk = 1; break;
+    default: break;
+    }
+}
+
 template <class PR, bool FACES>
 __device__ __forceinline__ void closed_pull(const BCtx<PR>& c, int cls, int fld, typename PR::T (&v)[19])
 {
     if (FACES && fld > 0) {
-        int di = 0, dj = 0, dk = 0;
-        switch (cls) {
-        case K_FACE_YT: dj = -1; break;
-        case K_FACE_Y1:
-        case K_OUTLET: dj = 1; break;
-        case K_FACE_MX1: di = 1; break;
-        case K_FACE_MXT: di = -1; break;
-        case K_FACE_ZT: dk = -1; break;
-        case K_FACE_Z1: dk = 1; break;
-        default: break;
-        }
+        int di, dj, dk;
+        face_copy_offset(cls, di, dj, dk);
         if (di | dj | dk) {
             pull_node(c, fld, c.b, c.i + di, c.j + dj, c.k + dk, v);
             return;
@@ -976,9 +1035,10 @@ __device__ __forceinline__ void boundary_lane(const StepPtrs& X, const Geom& G, 
 
     Rcur[fld * ps + c.g] = r;
     if (PR::kMoments) {
-        if (fld == 0) X.mcur[c.g] = make_float4((float)rho, (float)ux, (float)uy, (float)uz);
+        if (fld == 0) X.mcur[2 * (long long)c.g] = make_float4((float)rho, (float)ux, (float)uy, (float)uz);
         if (fld == 1)
-            X.mcur[ps + c.g] = make_float4((float)ca, (float)cb, (float)cc, u2_term((float)ux, (float)uy, (float)uz));
+            X.mcur[2 * (long long)c.g + 1] =
+                make_float4((float)ca, (float)cb, (float)cc, u2_term((float)ux, (float)uy, (float)uz));
     }
     if (write_macro) {
         Mac[(fld == 0 ? 0 : 3 + fld) * ps + c.g] = r;
@@ -990,18 +1050,197 @@ __device__ __forceinline__ void boundary_lane(const StepPtrs& X, const Geom& G, 
     }
 }
 
+// Direction 4K + lane of a group of four lanes (K a compile-time constant,
+// lane a run-time value): its lattice vector and weight, selected from the
+// compile-time tables.  Returns false past direction 18.
+template <int K>
+__device__ __forceinline__ bool lane_dir(int lane, int& q, int& ex, int& ey, int& ez, float& w)
+{
+    constexpr int q0 = 4 * K, q1 = 4 * K + 1 < 19 ? 4 * K + 1 : 18, q2 = 4 * K + 2 < 19 ? 4 * K + 2 : 18,
+                  q3 = 4 * K + 3 < 19 ? 4 * K + 3 : 18;
+    q = q0 + lane;
+    ex = lane == 0 ? EX(q0) : lane == 1 ? EX(q1) : lane == 2 ? EX(q2) : EX(q3);
+    ey = lane == 0 ? EY(q0) : lane == 1 ? EY(q1) : lane == 2 ? EY(q2) : EY(q3);
+    ez = lane == 0 ? EZ(q0) : lane == 1 ? EZ(q1) : lane == 2 ? EZ(q2) : EZ(q3);
+    w = (float)wq(q < 19 ? q : 18);
+    return q < 19;
+}
+
+// Boundary node g of the interleaved (FP32 / FP16-storage) forms with its
+// four lanes splitting the work three ways:
+//   1. directions: lane l pulls directions l, l+4, ... for all four fields
+//      (one vector load, one moment record and one polynomial per
+//      direction), species of a zero-gradient face from the interior
+//      neighbour, into the node's 76-value buffer in shared memory;
+//   2. fields: lane fld closes field fld (the same closures as
+//      boundary_lane) and forms its density; moments by shuffle;
+//   3. directions again: collide and store the four fields of each of its
+//      directions with one vector store.
+// The arithmetic of every value is that of boundary_lane and collide_store4.
+template <class PR, bool FACES>
+__device__ __forceinline__ void boundary_lane_lp(const StepPtrs& X, const Geom& G, const Phys& P, int write_macro,
+                                                 int g, int cls, int fld, unsigned mask, int lead, float* buf)
+{
+    using T = typename PR::T;
+    const typename PR::S* __restrict__ Pin = (const typename PR::S*)X.pin;
+    typename PR::S* __restrict__ Pout = (typename PR::S*)X.pout;
+    T* __restrict__ Rcur = (T*)X.rcur;
+    double* __restrict__ Mac = X.mac;
+    BCtx<PR> c;
+    c.Pin = Pin;
+    c.M = X.mprev;
+    c.Rprev = (const T*)X.rprev;
+    c.uin1 = (const T*)X.uin1;
+    c.uin2 = (const T*)X.uin2;
+    c.G = &G;
+    c.P = &P;
+    c.ps = G.ps;
+    c.g = g;
+    decode(G, c.g, c.b, c.i, c.j, c.k);
+    const long long ps = G.ps;
+    int di = 0, dj = 0, dk = 0;
+    if (FACES) face_copy_offset(cls, di, dj, dk);
+    const bool copy = (di | dj | dk) != 0;
+
+    // 1. pull by direction
+#define TMX_LANE_PULL(K)                                                                                         \
+    {                                                                                                            \
+        int q, ex, ey, ez;                                                                                       \
+        float w;                                                                                                 \
+        if (lane_dir<K>(fld, q, ex, ey, ez, w)) {                                                                \
+            T v[4] = {T(0), T(0), T(0), T(0)};                                                                   \
+            const int s0 = pull_src_e(G, c.b, c.i, c.j, c.k, ex, ey, ez);                                        \
+            if (s0 >= 0) PR::decode4(Pin, c.M, ps, q, ex, ey, ez, T(w), s0, v);                                 \
+            if (copy) {                                                                                          \
+                T u[4] = {T(0), T(0), T(0), T(0)};                                                               \
+                const int s1 = pull_src_e(G, c.b, c.i + di, c.j + dj, c.k + dk, ex, ey, ez);                     \
+                if (s1 >= 0) PR::decode4(Pin, c.M, ps, q, ex, ey, ez, T(w), s1, u);                             \
+                v[1] = u[1];                                                                                     \
+                v[2] = u[2];                                                                                     \
+                v[3] = u[3];                                                                                     \
+            }                                                                                                    \
+            buf[q] = v[0];                                                                                       \
+            buf[19 + q] = v[1];                                                                                  \
+            buf[38 + q] = v[2];                                                                                  \
+            buf[57 + q] = v[3];                                                                                  \
+        }                                                                                                        \
+    }
+    TMX_LANE_PULL(0)
+    TMX_LANE_PULL(1)
+    TMX_LANE_PULL(2)
+    TMX_LANE_PULL(3)
+    TMX_LANE_PULL(4)
+#undef TMX_LANE_PULL
+    __syncwarp(mask);
+
+    // 2. close by field
+    T v[19];
+#pragma unroll
+    for (int q = 0; q < 19; q++) v[q] = buf[fld * 19 + q];
+    if (!(copy && fld > 0)) {
+        if (FACES)
+            closure_face(c, cls, fld, v);
+        else
+            closure_edge(c, cls, fld, v);
+    }
+    T r = sum19(v);
+    T ux = T(0), uy = T(0), uz = T(0);
+    if (fld == 0) {
+        // the outlet row's density is pinned to rho_out (Tmixer.cpp:9575-9582)
+        if (c.b == 1 && c.j == 1) r = T(P.rho_out);
+        T sxm, sym, szm;
+        momentum(v, sxm, sym, szm);
+        ux = sxm / r;
+        uy = sym / r;
+        uz = szm / r;
+    }
+    ux = __shfl_sync(mask, ux, lead);
+    uy = __shfl_sync(mask, uy, lead);
+    uz = __shfl_sync(mask, uz, lead);
+    const T rho = __shfl_sync(mask, r, lead);
+    const T ca = __shfl_sync(mask, r, lead + 1);
+    const T cb = __shfl_sync(mask, r, lead + 2);
+    const T cc = __shfl_sync(mask, r, lead + 3);
+#pragma unroll
+    for (int q = 0; q < 19; q++) buf[fld * 19 + q] = v[q];
+    __syncwarp(mask);
+
+    // 3. collide and store by direction
+    const T rt = T(P.rateconst) * ca * cb;
+    const T rr[4] = {rho, ca, cb, cc};
+    T c1[4], c2[4];
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+        c1[m] = T(P.c1[m]);
+        c2[m] = T(P.c2[m]);
+    }
+#define TMX_LANE_STORE(K)                                                                                        \
+    {                                                                                                            \
+        int q, ex, ey, ez;                                                                                       \
+        float w;                                                                                                 \
+        if (lane_dir<K>(fld, q, ex, ey, ez, w)) {                                                                \
+            const T pw = PR::pw_dir(ex, ey, ez, T(w), ux, uy, uz);                                               \
+            T o[4], feq[4];                                                                                      \
+            _Pragma("unroll") for (int m = 0; m < 4; m++)                                                        \
+            {                                                                                                    \
+                feq[m] = PR::feq(rr[m], pw, q, false);                                                           \
+                o[m] = buf[m * 19 + q] * c1[m] + c2[m] * feq[m];                                                 \
+            }                                                                                                    \
+            o[1] = o[1] - T(w) * rt;                                                                             \
+            o[2] = o[2] - T(w) * rt;                                                                             \
+            o[3] = o[3] + (T(w) * rt) * T(2);                                                                    \
+            PR::encode4(Pout + PR::off(0, q, ps, c.g), o, feq);                                                  \
+        }                                                                                                        \
+    }
+    TMX_LANE_STORE(0)
+    TMX_LANE_STORE(1)
+    TMX_LANE_STORE(2)
+    TMX_LANE_STORE(3)
+    TMX_LANE_STORE(4)
+#undef TMX_LANE_STORE
+
+    Rcur[fld * ps + c.g] = r;
+    if (PR::kMoments) {
+        if (fld == 0) X.mcur[2 * (long long)c.g] = make_float4((float)rho, (float)ux, (float)uy, (float)uz);
+        if (fld == 1)
+            X.mcur[2 * (long long)c.g + 1] =
+                make_float4((float)ca, (float)cb, (float)cc, u2_term((float)ux, (float)uy, (float)uz));
+    }
+    if (write_macro) {
+        Mac[(fld == 0 ? 0 : 3 + fld) * ps + c.g] = r;
+        if (fld == 0) {
+            Mac[ps + c.g] = ux;
+            Mac[2 * ps + c.g] = uy;
+            Mac[3 * ps + c.g] = uz;
+        }
+    }
+}
+
+// Lane fld of boundary node g in the form's scheme; buf is the node's 76
+// values of shared memory (used by the interleaved forms).
+template <class PR, bool FACES>
+__device__ __forceinline__ void boundary_any(const StepPtrs& X, const Geom& G, const Phys& P, int write_macro, int g,
+                                             int cls, int fld, unsigned mask, int lead, float* buf)
+{
+    if constexpr (PR::kOnePass)
+        boundary_lane_lp<PR, FACES>(X, G, P, write_macro, g, cls, fld, mask, lead, buf);
+    else
+        boundary_lane<PR, FACES>(X, G, P, write_macro, g, cls, fld, mask, lead);
+}
+
 // One launch over a node list: thread 4t + fld is lane fld of node t.
 template <class PR, bool FACES>
 __device__ __forceinline__ void boundary_node(const StepPtrs& X, const int* __restrict__ bnode,
                                               const unsigned char* __restrict__ bcls, int nb, const Geom& G,
-                                              const Phys& P, int write_macro)
+                                              const Phys& P, int write_macro, float (*buf)[76])
 {
     const int gt = blockIdx.x * blockDim.x + threadIdx.x;
     const int t = gt >> 2, fld = gt & 3;
     // the four lanes of a node share one warp; whole nodes drop out together
     const unsigned mask = __ballot_sync(0xffffffffu, t < nb);
     if (t >= nb) return;
-    boundary_lane<PR, FACES>(X, G, P, write_macro, bnode[t], bcls[t], fld, mask, (threadIdx.x & 31) & ~3);
+    boundary_any<PR, FACES>(X, G, P, write_macro, bnode[t], bcls[t], fld, mask, (threadIdx.x & 31) & ~3,
+                            buf[threadIdx.x >> 2]);
 }
 
 // One interior node in the form's bulk scheme: one pass over the 76 values
@@ -1030,12 +1269,14 @@ __device__ __forceinline__ void bulk_any(const StepPtrs& X, const Geom& G, const
     __global__ void __launch_bounds__(kBoundaryThreads) k_bfaces_##NAME(                                       \
         StepPtrs X, const int* bnode, const unsigned char* bcls, int nb, Geom G, Phys P, int write_macro)       \
     {                                                                                                           \
-        boundary_node<PR, true>(X, bnode, bcls, nb, G, P, write_macro);                                         \
+        __shared__ float buf[kBoundaryThreads / 4][76];                                                         \
+        boundary_node<PR, true>(X, bnode, bcls, nb, G, P, write_macro, buf);                                    \
     }                                                                                                           \
     __global__ void __launch_bounds__(kBoundaryThreads) k_bedges_##NAME(                                       \
         StepPtrs X, const int* bnode, const unsigned char* bcls, int nb, Geom G, Phys P, int write_macro)       \
     {                                                                                                           \
-        boundary_node<PR, false>(X, bnode, bcls, nb, G, P, write_macro);                                        \
+        __shared__ float buf[kBoundaryThreads / 4][76];                                                         \
+        boundary_node<PR, false>(X, bnode, bcls, nb, G, P, write_macro, buf);                                   \
     }
 
 
@@ -1058,14 +1299,15 @@ __device__ __forceinline__ void bulk_any(const StepPtrs& X, const Geom& G, const
         int parity, int write_macro)                                                                            \
     {                                                                                                           \
         const int n = counts[WHICH];                                                                            \
+        __shared__ float buf[kBoundaryThreads / 4][76];                                                         \
         for (int base = blockIdx.x * blockDim.x; base < 4 * n; base += gridDim.x * blockDim.x) {                \
             const int t = (base + threadIdx.x) >> 2, fld = threadIdx.x & 3;                                     \
             const unsigned mask = __ballot_sync(0xffffffffu, t < n);                                            \
             if (t < n) {                                                                                        \
                 const int2 e = list[t];                                                                         \
                 const MixerDesc& d = D[e.y >> 8];                                                               \
-                boundary_lane<PR, FACES>(d.X[parity], d.G, d.P, write_macro, e.x, e.y & 255, fld, mask,         \
-                                         (threadIdx.x & 31) & ~3);                                              \
+                boundary_any<PR, FACES>(d.X[parity], d.G, d.P, write_macro, e.x, e.y & 255, fld, mask,          \
+                                        (threadIdx.x & 31) & ~3, buf[threadIdx.x >> 2]);                        \
             }                                                                                                   \
         }                                                                                                       \
     }
