@@ -118,11 +118,12 @@ __device__ __forceinline__ double div_c(double x, double d, double r)
     return __fma_rn(e, r, q);
 }
 
+// q may be a run-time value: the constants are selected, not branched on
 __device__ __forceinline__ double feq_div(double x, int q)
 {
-    if (q == 0) return div_c(x, 3.0, 1.0 / 3.0);
-    if (q <= 6) return div_c(x, 18.0, 1.0 / 18.0);
-    return div_c(x, 36.0, 1.0 / 36.0);
+    const double d = q == 0 ? 3.0 : (q <= 6 ? 18.0 : 36.0);
+    const double r = q == 0 ? 1.0 / 3.0 : (q <= 6 ? 1.0 / 18.0 : 1.0 / 36.0);
+    return div_c(x, d, r);
 }
 
 __device__ __forceinline__ double feq_div_exact(double x, int q)

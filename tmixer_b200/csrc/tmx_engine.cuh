@@ -64,6 +64,24 @@ __device__ __forceinline__ float poly_q_rn(int q, float ux, float uy, float uz)
     return poly_q_rn_t(q, ux, uy, uz, u2_term(ux, uy, uz));
 }
 
+// Collision of one direction of the interleaved forms with sm_100's packed
+// two-wide FP32 arithmetic, on the field pairs (flow, A) and (B, C): given
+// the pulled values, the densities, w_q * poly_q (pw) and w_q * rate (wrt),
+// the equilibria f = r * pw and the post-collision values
+// o = in * c1 + c2 * f, A and B minus wrt, C plus 2 wrt.
+__device__ __forceinline__ void collide_pairs(float2 in01, float2 in23, float2 r01, float2 r23, float pw, float2 c1a,
+                                              float2 c1b, float2 c2a, float2 c2b, float wrt, float2& o01, float2& o23,
+                                              float2& f01, float2& f23)
+{
+    const float2 pp = make_float2(pw, pw);
+    f01 = __fmul2_rn(r01, pp);
+    f23 = __fmul2_rn(r23, pp);
+    o01 = __ffma2_rn(c2a, f01, __fmul2_rn(in01, c1a));
+    o23 = __ffma2_rn(c2b, f23, __fmul2_rn(in23, c1b));
+    o01 = __fadd2_rn(o01, make_float2(0.0f, -wrt));
+    o23 = __fadd2_rn(o23, make_float2(-wrt, 2.0f * wrt));
+}
+
 // Plain form: FP64 storage and arithmetic, operation by operation as the
 // reference (the translation unit is compiled with --fmad=false); the
 // equilibrium divisions are correctly rounded (div_c).
@@ -87,6 +105,45 @@ struct F64 {
     __device__ static T decode(const S* p, int, int, const float4*, long long, int) { return __ldg(p); }
     __device__ static void encode(S* p, T v, T) { *p = v; }
     __device__ static T raw(const S* p) { return __ldg(p); }
+    // the equilibrium polynomial of one direction given by (ex, ey, ez), with
+    // the operations of eq_poly (the weight enters through feq's division)
+    __device__ static T pw_dir(int ex, int ey, int ez, T, T ux, T uy, T uz)
+    {
+        const T u2 = ux * ux + uy * uy + uz * uz;
+        const T t = T(3) * u2 / T(2);
+        if ((ex | ey | ez) == 0) return T(1) - t;
+        const T eu = e_dot_u_e(ex, ey, ez, ux, uy, uz);
+        return T(1) + T(3) * eu - t + T(9) * eu * eu / T(2);
+    }
+    // fields first .. last-1 of direction q pulled from node s (one plane each)
+    __device__ static void decode_fields(const S* __restrict__ Pin, const float4* __restrict__, long long ps, int q,
+                                         int, int, int, T, int s, T (&v)[4], int first, int last)
+    {
+#pragma unroll
+        for (int m = 0; m < 4; m++)
+            if (m >= first && m < last) v[m] = __ldg(Pin + off(m, q, ps, s));
+    }
+    __device__ static void store4(S* __restrict__ Pout, int q, long long ps, int g, const T (&v)[4], const T (&)[4])
+    {
+#pragma unroll
+        for (int m = 0; m < 4; m++) Pout[off(m, q, ps, g)] = v[m];
+    }
+    // collide and store the four fields of direction q (collide_store's
+    // operations, per field)
+    __device__ static void collide_dir(S* __restrict__ Pout, int q, long long ps, int g, const T (&in)[4],
+                                       const T (&r)[4], T pw, const T (&c1)[4], const T (&c2)[4], T w, T rt)
+    {
+        T o[4], f[4];
+#pragma unroll
+        for (int m = 0; m < 4; m++) {
+            f[m] = feq(r[m], pw, q, tiny(r[m]));
+            o[m] = in[m] * c1[m] + c2[m] * f[m];
+        }
+        o[1] = o[1] - w * rt;
+        o[2] = o[2] - w * rt;
+        o[3] = o[3] + (w * rt) * T(2);
+        store4(Pout, q, ps, g, o, f);
+    }
 };
 
 // FP32 arithmetic and storage.
@@ -113,6 +170,10 @@ struct F32 {
     {
         *(float4*)p = make_float4(v[0], v[1], v[2], v[3]);
     }
+    __device__ static void store4(S* Pout, int q, long long ps, int g, const T (&v)[4], const T (&feq)[4])
+    {
+        encode4(Pout + off(0, q, ps, g), v, feq);
+    }
     // poly holds w_q * poly_q, so that an equilibrium value is one multiply
     __device__ static void poly(T ux, T uy, T uz, T (&p)[19])
     {
@@ -131,11 +192,43 @@ struct F32 {
         const T eu = e_dot_u_e(ex, ey, ez, ux, uy, uz);
         return (T(1) + T(3) * eu - t + T(9) * eu * eu / T(2)) * w;
     }
-    // the four fields pulled from source s along (ex, ey, ez) of direction q
+    // the four fields pulled from source s along (ex, ey, ez) of direction q,
+    // as the pairs (flow, A), (B, C)
+    __device__ static void decode_pairs(const S* __restrict__ Pin, const float4* __restrict__, long long ps, int q, int,
+                                        int, int, T, int s, float2& v01, float2& v23)
+    {
+        const float4 x = __ldg((const float4*)(Pin + off(0, q, ps, s)));
+        v01 = make_float2(x.x, x.y);
+        v23 = make_float2(x.z, x.w);
+    }
     __device__ static void decode4(const S* __restrict__ Pin, const float4* __restrict__, long long ps, int q, int,
                                    int, int, T, int s, T (&v)[4])
     {
         load4(Pin + off(0, q, ps, s), v);
+    }
+    __device__ static void store_pairs(S* Pout, int q, long long ps, int g, float2 o01, float2 o23, float2, float2)
+    {
+        *(float4*)(Pout + off(0, q, ps, g)) = make_float4(o01.x, o01.y, o23.x, o23.y);
+    }
+    // collide and store the four fields of direction q (packed pairs)
+    __device__ static void collide_dir(S* Pout, int q, long long ps, int g, const T (&in)[4], const T (&r)[4], T pw,
+                                       const T (&c1)[4], const T (&c2)[4], T w, T rt)
+    {
+        float2 o01, o23, f01, f23;
+        collide_pairs(make_float2(in[0], in[1]), make_float2(in[2], in[3]), make_float2(r[0], r[1]),
+                      make_float2(r[2], r[3]), pw, make_float2(c1[0], c1[1]), make_float2(c1[2], c1[3]),
+                      make_float2(c2[0], c2[1]), make_float2(c2[2], c2[3]), w * rt, o01, o23, f01, f23);
+        store_pairs(Pout, q, ps, g, o01, o23, f01, f23);
+    }
+    // fields first .. last-1 (one vector access brings all four)
+    __device__ static void decode_fields(const S* __restrict__ Pin, const float4* __restrict__ M, long long ps, int q,
+                                         int ex, int ey, int ez, T w, int s, T (&v)[4], int first, int last)
+    {
+        T u[4];
+        decode4(Pin, M, ps, q, ex, ey, ez, w, s, u);
+#pragma unroll
+        for (int m = 0; m < 4; m++)
+            if (m >= first && m < last) v[m] = u[m];
     }
     __device__ static T decode(const S* p, int, int, const float4*, long long, int) { return __ldg(p); }
     __device__ static void encode(S* p, T v, T) { *p = v; }
@@ -176,6 +269,10 @@ struct F16 {
         x.y = *(const unsigned*)&hi;
         *(uint2*)p = x;
     }
+    __device__ static void store4(S* Pout, int q, long long ps, int g, const T (&v)[4], const T (&feq)[4])
+    {
+        encode4(Pout + off(0, q, ps, g), v, feq);
+    }
     // poly holds w_q * poly_q (rounded as below), so that an equilibrium
     // value is one multiply
     __device__ static void poly(T ux, T uy, T uz, T (&p)[19])
@@ -194,16 +291,58 @@ struct F16 {
     {
         return __fmul_rn(poly_e_rn_t(ex, ey, ez, ux, uy, uz, u2_term(ux, uy, uz)), w);
     }
+    // the four fields pulled from source s along (ex, ey, ez) of direction q,
+    // as the pairs (flow, A), (B, C): the stored part plus the writer's
+    // equilibrium, each product and sum rounded on its own
+    __device__ static void decode_pairs(const S* __restrict__ Pin, const float4* __restrict__ M, long long ps, int q,
+                                        int ex, int ey, int ez, T w, int s, float2& v01, float2& v23)
+    {
+        const uint2 x = __ldg((const uint2*)(Pin + off(0, q, ps, s)));
+        const float2 raw01 = __half22float2(*(const __half2*)&x.x), raw23 = __half22float2(*(const __half2*)&x.y);
+        const float4 mf = __ldg(M + 2 * (long long)s), ms = __ldg(M + 2 * (long long)s + 1);
+        const float pw = __fmul_rn(poly_e_rn_t(ex, ey, ez, mf.y, mf.z, mf.w, ms.w), w);
+        const float2 pp = make_float2(pw, pw);
+        v01 = __fadd2_rn(raw01, __fmul2_rn(make_float2(mf.x, ms.x), pp));
+        v23 = __fadd2_rn(raw23, __fmul2_rn(make_float2(ms.y, ms.z), pp));
+    }
     __device__ static void decode4(const S* __restrict__ Pin, const float4* __restrict__ M, long long ps, int q,
                                    int ex, int ey, int ez, T w, int s, T (&v)[4])
     {
-        load4(Pin + off(0, q, ps, s), v);
-        const float4 mf = __ldg(M + 2 * (long long)s), ms = __ldg(M + 2 * (long long)s + 1);
-        const float pw = __fmul_rn(poly_e_rn_t(ex, ey, ez, mf.y, mf.z, mf.w, ms.w), w);
-        v[0] = v[0] + feq(mf.x, pw, q, false);
-        v[1] = v[1] + feq(ms.x, pw, q, false);
-        v[2] = v[2] + feq(ms.y, pw, q, false);
-        v[3] = v[3] + feq(ms.z, pw, q, false);
+        float2 a, b;
+        decode_pairs(Pin, M, ps, q, ex, ey, ez, w, s, a, b);
+        v[0] = a.x;
+        v[1] = a.y;
+        v[2] = b.x;
+        v[3] = b.y;
+    }
+    __device__ static void store_pairs(S* Pout, int q, long long ps, int g, float2 o01, float2 o23, float2 f01,
+                                       float2 f23)
+    {
+        const __half2 lo = __float22half2_rn(__fadd2_rn(o01, make_float2(-f01.x, -f01.y)));
+        const __half2 hi = __float22half2_rn(__fadd2_rn(o23, make_float2(-f23.x, -f23.y)));
+        uint2 x;
+        x.x = *(const unsigned*)&lo;
+        x.y = *(const unsigned*)&hi;
+        *(uint2*)(Pout + off(0, q, ps, g)) = x;
+    }
+    // collide and store the four fields of direction q (packed pairs)
+    __device__ static void collide_dir(S* Pout, int q, long long ps, int g, const T (&in)[4], const T (&r)[4], T pw,
+                                       const T (&c1)[4], const T (&c2)[4], T w, T rt)
+    {
+        float2 o01, o23, f01, f23;
+        collide_pairs(make_float2(in[0], in[1]), make_float2(in[2], in[3]), make_float2(r[0], r[1]),
+                      make_float2(r[2], r[3]), pw, make_float2(c1[0], c1[1]), make_float2(c1[2], c1[3]),
+                      make_float2(c2[0], c2[1]), make_float2(c2[2], c2[3]), w * rt, o01, o23, f01, f23);
+        store_pairs(Pout, q, ps, g, o01, o23, f01, f23);
+    }
+    __device__ static void decode_fields(const S* __restrict__ Pin, const float4* __restrict__ M, long long ps, int q,
+                                         int ex, int ey, int ez, T w, int s, T (&v)[4], int first, int last)
+    {
+        T u[4];
+        decode4(Pin, M, ps, q, ex, ey, ez, w, s, u);
+#pragma unroll
+        for (int m = 0; m < 4; m++)
+            if (m >= first && m < last) v[m] = u[m];
     }
     __device__ static T decode(const S* p, int fld, int q, const float4* M, long long, int src)
     {
@@ -459,35 +598,39 @@ __device__ __forceinline__ void bulk_node_lp(const StepPtrs& X, const Geom& G, c
     const int sy = box_nx(G, b), sz = box_nx(G, b) * box_ny(G, b);
     const int iface = (b == 0 && j == 1) ? 1 : ((b == 1 && j == G.mny) ? 2 : 0);
 
-    T f[19], a[19], bb[19], c[19];
+    // the four fields as the pairs (flow, A), (B, C)
+    float2 p01[19], p23[19];
 #pragma unroll
     for (int q = 0; q < 19; q++) {
         const int s = bulk_src(G, g, i, k, sy, sz, iface, q);
-        T raw[4];
-        PR::load4(Pin + PR::off(0, q, ps, s), raw);
-        T e0 = T(0), e1 = T(0), e2 = T(0), e3 = T(0);
-        if constexpr (PR::kMoments) {
-            const float4 mf = __ldg(M + 2 * (long long)s), ms = __ldg(M + 2 * (long long)s + 1);
-            const float pq = PR::src_pw(q, mf, ms);
-            e0 = PR::feq(mf.x, pq, q, false);
-            e1 = PR::feq(ms.x, pq, q, false);
-            e2 = PR::feq(ms.y, pq, q, false);
-            e3 = PR::feq(ms.z, pq, q, false);
-        }
-        f[q] = raw[0] + e0;
-        a[q] = raw[1] + e1;
-        bb[q] = raw[2] + e2;
-        c[q] = raw[3] + e3;
+        PR::decode_pairs(Pin, M, ps, q, EX(q), EY(q), EZ(q), (float)wq(q), s, p01[q], p23[q]);
     }
-    const T rho = sum19(f);
+    // sums in index order, two fields at a time
+    float2 s01 = p01[0], s23 = p23[0];
+#pragma unroll
+    for (int q = 1; q < 19; q++) {
+        s01 = __fadd2_rn(s01, p01[q]);
+        s23 = __fadd2_rn(s23, p23[q]);
+    }
+    const T rho = s01.x, ca = s01.y, cb = s23.x, cc = s23.y;
+    T f[19];
+#pragma unroll
+    for (int q = 0; q < 19; q++) f[q] = p01[q].x;
     T sxm, sym, szm;
     momentum(f, sxm, sym, szm);
     const T ux = sxm / rho, uy = sym / rho, uz = szm / rho;
     T poly[19];
     PR::poly(ux, uy, uz, poly);
-    const T ca = sum19(a), cb = sum19(bb), cc = sum19(c);
     const T rt = T(P.rateconst) * ca * cb;
-    collide_store4<PR>(Pout, ps, g, f, a, bb, c, rho, ca, cb, cc, poly, P, rt);
+    const float2 r01 = make_float2(rho, ca), r23 = make_float2(cb, cc);
+    const float2 c1a = make_float2((float)P.c1[0], (float)P.c1[1]), c1b = make_float2((float)P.c1[2], (float)P.c1[3]);
+    const float2 c2a = make_float2((float)P.c2[0], (float)P.c2[1]), c2b = make_float2((float)P.c2[2], (float)P.c2[3]);
+#pragma unroll
+    for (int q = 0; q < 19; q++) {
+        float2 o01, o23, f01, f23;
+        collide_pairs(p01[q], p23[q], r01, r23, poly[q], c1a, c1b, c2a, c2b, (float)wq(q) * rt, o01, o23, f01, f23);
+        PR::store_pairs(Pout, q, ps, g, o01, o23, f01, f23);
+    }
     if (b == 0 && j == 2 && (i == G.ia || i == G.ib)) {
         T* Rcur = (T*)X.rcur;
         Rcur[g] = rho;
@@ -1054,7 +1197,7 @@ __device__ __forceinline__ void boundary_lane(const StepPtrs& X, const Geom& G, 
 // lane a run-time value): its lattice vector and weight, selected from the
 // compile-time tables.  Returns false past direction 18.
 template <int K>
-__device__ __forceinline__ bool lane_dir(int lane, int& q, int& ex, int& ey, int& ez, float& w)
+__device__ __forceinline__ bool lane_dir(int lane, int& q, int& ex, int& ey, int& ez, double& w)
 {
     constexpr int q0 = 4 * K, q1 = 4 * K + 1 < 19 ? 4 * K + 1 : 18, q2 = 4 * K + 2 < 19 ? 4 * K + 2 : 18,
                   q3 = 4 * K + 3 < 19 ? 4 * K + 3 : 18;
@@ -1062,12 +1205,11 @@ __device__ __forceinline__ bool lane_dir(int lane, int& q, int& ex, int& ey, int
     ex = lane == 0 ? EX(q0) : lane == 1 ? EX(q1) : lane == 2 ? EX(q2) : EX(q3);
     ey = lane == 0 ? EY(q0) : lane == 1 ? EY(q1) : lane == 2 ? EY(q2) : EY(q3);
     ez = lane == 0 ? EZ(q0) : lane == 1 ? EZ(q1) : lane == 2 ? EZ(q2) : EZ(q3);
-    w = (float)wq(q < 19 ? q : 18);
+    w = wq(q < 19 ? q : 18);
     return q < 19;
 }
 
-// Boundary node g of the interleaved (FP32 / FP16-storage) forms with its
-// four lanes splitting the work three ways:
+// Boundary node g with its four lanes splitting the work three ways:
 //   1. directions: lane l pulls directions l, l+4, ... for all four fields
 //      (one vector load, one moment record and one polynomial per
 //      direction), species of a zero-gradient face from the interior
@@ -1076,10 +1218,13 @@ __device__ __forceinline__ bool lane_dir(int lane, int& q, int& ex, int& ey, int
 //      boundary_lane) and forms its density; moments by shuffle;
 //   3. directions again: collide and store the four fields of each of its
 //      directions with one vector store.
-// The arithmetic of every value is that of boundary_lane and collide_store4.
+// Every value is computed with the operations, in the order, of the
+// one-field-per-thread step (pull_node, the closures, sum19, momentum,
+// collide_store), so the FP64 form stays bit-exact.
 template <class PR, bool FACES>
 __device__ __forceinline__ void boundary_lane_lp(const StepPtrs& X, const Geom& G, const Phys& P, int write_macro,
-                                                 int g, int cls, int fld, unsigned mask, int lead, float* buf)
+                                                 int g, int cls, int fld, unsigned mask, int lead,
+                                                 typename PR::T* buf)
 {
     using T = typename PR::T;
     const typename PR::S* __restrict__ Pin = (const typename PR::S*)X.pin;
@@ -1106,18 +1251,15 @@ __device__ __forceinline__ void boundary_lane_lp(const StepPtrs& X, const Geom& 
 #define TMX_LANE_PULL(K)                                                                                         \
     {                                                                                                            \
         int q, ex, ey, ez;                                                                                       \
-        float w;                                                                                                 \
+        double w;                                                                                                \
         if (lane_dir<K>(fld, q, ex, ey, ez, w)) {                                                                \
             T v[4] = {T(0), T(0), T(0), T(0)};                                                                   \
             const int s0 = pull_src_e(G, c.b, c.i, c.j, c.k, ex, ey, ez);                                        \
-            if (s0 >= 0) PR::decode4(Pin, c.M, ps, q, ex, ey, ez, T(w), s0, v);                                 \
+            /* a zero-gradient face takes its species from the interior neighbour */                             \
+            if (s0 >= 0) PR::decode_fields(Pin, c.M, ps, q, ex, ey, ez, T(w), s0, v, 0, copy ? 1 : 4);           \
             if (copy) {                                                                                          \
-                T u[4] = {T(0), T(0), T(0), T(0)};                                                               \
                 const int s1 = pull_src_e(G, c.b, c.i + di, c.j + dj, c.k + dk, ex, ey, ez);                     \
-                if (s1 >= 0) PR::decode4(Pin, c.M, ps, q, ex, ey, ez, T(w), s1, u);                             \
-                v[1] = u[1];                                                                                     \
-                v[2] = u[2];                                                                                     \
-                v[3] = u[3];                                                                                     \
+                if (s1 >= 0) PR::decode_fields(Pin, c.M, ps, q, ex, ey, ez, T(w), s1, v, 1, 4);                  \
             }                                                                                                    \
             buf[q] = v[0];                                                                                       \
             buf[19 + q] = v[1];                                                                                  \
@@ -1177,19 +1319,10 @@ __device__ __forceinline__ void boundary_lane_lp(const StepPtrs& X, const Geom& 
 #define TMX_LANE_STORE(K)                                                                                        \
     {                                                                                                            \
         int q, ex, ey, ez;                                                                                       \
-        float w;                                                                                                 \
+        double w;                                                                                                \
         if (lane_dir<K>(fld, q, ex, ey, ez, w)) {                                                                \
-            const T pw = PR::pw_dir(ex, ey, ez, T(w), ux, uy, uz);                                               \
-            T o[4], feq[4];                                                                                      \
-            _Pragma("unroll") for (int m = 0; m < 4; m++)                                                        \
-            {                                                                                                    \
-                feq[m] = PR::feq(rr[m], pw, q, false);                                                           \
-                o[m] = buf[m * 19 + q] * c1[m] + c2[m] * feq[m];                                                 \
-            }                                                                                                    \
-            o[1] = o[1] - T(w) * rt;                                                                             \
-            o[2] = o[2] - T(w) * rt;                                                                             \
-            o[3] = o[3] + (T(w) * rt) * T(2);                                                                    \
-            PR::encode4(Pout + PR::off(0, q, ps, c.g), o, feq);                                                  \
+            const T in[4] = {buf[q], buf[19 + q], buf[38 + q], buf[57 + q]};                                     \
+            PR::collide_dir(Pout, q, ps, c.g, in, rr, PR::pw_dir(ex, ey, ez, T(w), ux, uy, uz), c1, c2, T(w), rt); \
         }                                                                                                        \
     }
     TMX_LANE_STORE(0)
@@ -1216,23 +1349,19 @@ __device__ __forceinline__ void boundary_lane_lp(const StepPtrs& X, const Geom& 
     }
 }
 
-// Lane fld of boundary node g in the form's scheme; buf is the node's 76
-// values of shared memory (used by the interleaved forms).
+// Lane fld of boundary node g; buf is the node's 76 values of shared memory.
 template <class PR, bool FACES>
 __device__ __forceinline__ void boundary_any(const StepPtrs& X, const Geom& G, const Phys& P, int write_macro, int g,
-                                             int cls, int fld, unsigned mask, int lead, float* buf)
+                                             int cls, int fld, unsigned mask, int lead, typename PR::T* buf)
 {
-    if constexpr (PR::kOnePass)
-        boundary_lane_lp<PR, FACES>(X, G, P, write_macro, g, cls, fld, mask, lead, buf);
-    else
-        boundary_lane<PR, FACES>(X, G, P, write_macro, g, cls, fld, mask, lead);
+    boundary_lane_lp<PR, FACES>(X, G, P, write_macro, g, cls, fld, mask, lead, buf);
 }
 
 // One launch over a node list: thread 4t + fld is lane fld of node t.
 template <class PR, bool FACES>
 __device__ __forceinline__ void boundary_node(const StepPtrs& X, const int* __restrict__ bnode,
                                               const unsigned char* __restrict__ bcls, int nb, const Geom& G,
-                                              const Phys& P, int write_macro, float (*buf)[76])
+                                              const Phys& P, int write_macro, typename PR::T (*buf)[76])
 {
     const int gt = blockIdx.x * blockDim.x + threadIdx.x;
     const int t = gt >> 2, fld = gt & 3;
@@ -1269,13 +1398,13 @@ __device__ __forceinline__ void bulk_any(const StepPtrs& X, const Geom& G, const
     __global__ void __launch_bounds__(kBoundaryThreads) k_bfaces_##NAME(                                       \
         StepPtrs X, const int* bnode, const unsigned char* bcls, int nb, Geom G, Phys P, int write_macro)       \
     {                                                                                                           \
-        __shared__ float buf[kBoundaryThreads / 4][76];                                                         \
+        __shared__ PR::T buf[kBoundaryThreads / 4][76];                                                            \
         boundary_node<PR, true>(X, bnode, bcls, nb, G, P, write_macro, buf);                                    \
     }                                                                                                           \
     __global__ void __launch_bounds__(kBoundaryThreads) k_bedges_##NAME(                                       \
         StepPtrs X, const int* bnode, const unsigned char* bcls, int nb, Geom G, Phys P, int write_macro)       \
     {                                                                                                           \
-        __shared__ float buf[kBoundaryThreads / 4][76];                                                         \
+        __shared__ PR::T buf[kBoundaryThreads / 4][76];                                                            \
         boundary_node<PR, false>(X, bnode, bcls, nb, G, P, write_macro, buf);                                   \
     }
 
@@ -1299,7 +1428,7 @@ __device__ __forceinline__ void bulk_any(const StepPtrs& X, const Geom& G, const
         int parity, int write_macro)                                                                            \
     {                                                                                                           \
         const int n = counts[WHICH];                                                                            \
-        __shared__ float buf[kBoundaryThreads / 4][76];                                                         \
+        __shared__ PR::T buf[kBoundaryThreads / 4][76];                                                            \
         for (int base = blockIdx.x * blockDim.x; base < 4 * n; base += gridDim.x * blockDim.x) {                \
             const int t = (base + threadIdx.x) >> 2, fld = threadIdx.x & 3;                                     \
             const unsigned mask = __ballot_sync(0xffffffffu, t < n);                                            \
