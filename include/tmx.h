@@ -159,6 +159,25 @@ int tmx_mixing(tmx_handle *h, double *rows_out, double *outlet_im);
  *     by the caller. */
 int tmx_mixing_static(tmx_handle *h, double *rows_out, double *outlet_im);
 
+/* Pressure and specific power after the last step: the numbers
+ * write_Pressure_Power() prints (Tmixer.cpp:9866-10027), in lattice units,
+ * computed in FP64 on the device in the reference's summation order.
+ *   pressure_rows[(mny+iny)*3]  {row, p, p - p_top}: p = mean density / 3 over
+ *       mixing row 1..mny, then inlet row 1..iny over x = ia..ib (row number
+ *       j + mny); p_top = the same over inlet row iny
+ *   pressure_x[inx*2]           {i, p}: mean density / 3 over the inlet box's
+ *       cross-section at x = i
+ *   power_rows[(mny-2)*5]       {j, cross-section rate, total rate, the same
+ *       two summed over every x}: 2 vis <deformation rate> over mixing row
+ *       j = 2..mny-1 (vis = (2 tau - 1)/6).  The first two reproduce the
+ *       reference, whose x loop assigns instead of adding (only x = mnx-1
+ *       enters its sums); the last two add every x.
+ *   units[2]                    the reference's factors P0 and Pw0 (its
+ *       Tmixer.cpp:189-196 with length = inx) that turn p and the rates into
+ *       pascal and W/kg as it prints them. */
+int tmx_pressure_power(tmx_handle *h, double *pressure_rows, double *pressure_x, double *power_rows,
+                       double units[2]);
+
 /* FP64 totals over both boxes after the last step: out[0] = sum rho,
  * out[1..3] = sum cA, cB, cC, out[4] = sum (cA + cB + cC), out[5] = outlet
  * flux sum(rho*uy) over mixing row 1, out[6] = number of non-finite values in

@@ -14,7 +14,8 @@ Substitutions (each one a parameter of the case, not a change of algorithm):
     reference uses, and the only form that opens ``mnx`` columns for even widths;
   * ``amax``/``bmax``/``sumy*`` start at 0 (Tmixer.cpp:10171-10175 read them
     uninitialised);
-  * the mixing-quality rows print 17 significant digits instead of ``%g``
+  * the mixing-quality and pressure/power rows print 17 significant digits
+    instead of ``%g``
     (Tmixer.cpp:10300-10401);
   * the reference ``main`` (Tmixer.cpp:10413) is renamed so the harness drives
     the phase functions itself.
@@ -91,6 +92,10 @@ def patched_source(params: dict) -> str:
         raise RuntimeError("expected 4 mixing-quality formats, found %d" % n)
     src = src.replace('"%d\\t%g\\t%g\\t%g\\t%g\\t%g\\t%g\\n"',
                       '"%d\\t%.17g\\t%.17g\\t%.17g\\t%.17g\\t%.17g\\t%.17g\\n"')
+    n = src.count('"%d\\t%g\\t%g\\t%g\\n"')
+    if n != 4:
+        raise RuntimeError("expected 4 pressure/power formats, found %d" % n)
+    src = src.replace('"%d\\t%g\\t%g\\t%g\\n"', '"%d\\t%.17g\\t%.17g\\t%.17g\\n"')
     sub1("int main()\n", "int tmx_reference_main_unused()\n")
     with open(HARNESS, "r") as fh:
         src += "\n" + fh.read()

@@ -54,6 +54,7 @@ def lib():
         L.orc_fields.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
         L.orc_pops.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
         L.orc_mixing.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.orc_pressure_power.argtypes = [ctypes.c_void_p] * 5
         L.orc_inlet_profile.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         L.orc_collide_preview.argtypes = [ctypes.c_void_p]
         L.orc_fn.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
@@ -118,6 +119,17 @@ class Oracle:
         lib().orc_mixing(self._h, rows.ctypes.data)
         return rows
 
+    def pressure_power(self):
+        """(pressure rows (mny+iny, 3), cross-section pressures (inx, 2),
+        power rows (mny-2, 5), units (P0, Pw0)) as orc_pressure_power."""
+        c = self.case
+        prow = np.empty((c["mny"] + c["iny"], 3))
+        px = np.empty((c["inx"], 2))
+        pw = np.empty((c["mny"] - 2, 5))
+        units = np.empty(2)
+        lib().orc_pressure_power(self._h, prow.ctypes.data, px.ctypes.data, pw.ctypes.data, units.ctypes.data)
+        return prow, px, pw, units
+
     def inlet_profile(self):
         n = (self.case["iny"] + 3, self.case["nz"] + 3)
         u1 = np.empty(n, dtype=np.float64)
@@ -173,6 +185,22 @@ def read_ref_mixing(path: str) -> np.ndarray:
     return np.array(rows, dtype=np.float64)
 
 
+def read_ref_pressure(path: str) -> dict:
+    """The three zones of the reference's Pressure_<steps>.dat as arrays of
+    rows {index, value, value * unit, third column}."""
+    zones, cur = {}, None
+    with open(path) as fh:
+        for line in fh:
+            if line.startswith("ZONE"):
+                cur = line.split('"')[1]
+                zones[cur] = []
+                continue
+            parts = line.split()
+            if cur and len(parts) == 4:
+                zones[cur].append([float(x) for x in parts])
+    return {k: np.array(v, dtype=np.float64) for k, v in zones.items()}
+
+
 def run_ref(binary: str, steps: int, with_pops: bool = False, threads: int | None = None, warmup: int = 0):
     """Run a reference binary in a scratch directory; return (dump, mixing
     rows, seconds of the timed loop: the steps after the first ``warmup``)."""
@@ -190,4 +218,5 @@ def run_ref(binary: str, steps: int, with_pops: bool = False, threads: int | Non
                 secs = float(line.split()[1])
         dump = read_ref_dump(os.path.join(d, "out.bin"), with_pops)
         mix = read_ref_mixing(os.path.join(d, "MixingQuality_%d.dat" % steps))
+        dump["pressure"] = read_ref_pressure(os.path.join(d, "Pressure_%d.dat" % steps))
     return dump, mix, secs

@@ -16,6 +16,7 @@
  *   calculate_velocity_density     Tmixer.cpp:9352-9656
  *   collision                      Tmixer.cpp:9661-9860
  *   write_MixingQuality (numbers)  Tmixer.cpp:10161-10409
+ *   write_Pressure_Power (numbers) Tmixer.cpp:9866-10027
  * with the same array semantics: two boxes (inlet "I" = box 0, mixing "M" =
  * box 1), each padded with ghost planes 0 and n+1 (allocated to n+2), z the
  * contiguous axis; four fields (flow f, species A g, B h, C p).
@@ -1151,6 +1152,113 @@ void orc_mixing(const orc_t *S, double *rows)
                     r[4 + s] = 0.0;
             }
         }
+    }
+}
+
+/* Pressure and specific power, Tmixer.cpp:9866-10027 (the numbers it prints),
+ * in lattice units, with the reference's unit factors:
+ *   prow[(mny+iny)*3]  {row, p, p - p_top}: p = mean density / 3 over mixing
+ *                      row j=1..mny (x=1..mnx), then inlet row j=1..iny
+ *                      (x=ia..ib, divided by nz*mnx as the reference does);
+ *                      p_top = the same over inlet row iny (:9895-9905)
+ *   px[inx*2]          {i, p}: mean density / 3 over the inlet cross-section x=i
+ *   pw[(mny-2)*5]      {j, cross-section rate, total rate, the same two summed
+ *                      over every column}: for j=2..mny-1 the reference's loop
+ *                      (:9985-10024) assigns the per-column rates inside the
+ *                      x loop, so only column mnx-1 reaches the k sums; the
+ *                      last two entries add every column instead
+ *   units[2]           P0 and Pw0 (Tmixer.cpp:189-196), the factors the
+ *                      reference multiplies the printed values by */
+void orc_pressure_power(const orc_t *S, double *prow, double *px, double *pw, double *units)
+{
+    const int nz = S->nz, mnx = S->P.mnx, mny = S->P.mny, iny = S->P.iny, inx = S->P.inx, ia = S->P.ia;
+    const double *ri = S->rho[0][0], *rm = S->rho[1][0];
+    const double *ux = S->u[1][0], *uy = S->u[1][1], *uz = S->u[1][2];
+    const double tau = S->P.tau, rho0 = S->P.rho0;
+    /* unit factors as the reference's macros expand (length = inx) */
+    const double L0 = (0.0008 / (inx - 1));
+    const double T0 = ((((2.0 * tau - 1.0) / 6.0) / 0.000001004) * (L0 * L0));
+    const double M0 = ((101325.0 / (rho0 / 3.0)) * (L0 * T0 * T0));
+    units[0] = ((M0) / (L0 * T0 * T0));
+    units[1] = ((L0 * L0) / (T0 * T0 * T0));
+    const double vis = ((2.0 * tau - 1.0) / 6.0) * (1.0 * 1.0 * 1.0);
+
+    double sumx = 0;
+    for (int i = 1; i <= mnx; i++) {
+        double sumz = 0;
+        for (int k = 1; k <= nz; k++) sumz += ri[IX(S, 0, i + ia - 1, iny, k)];
+        sumx += sumz;
+    }
+    const double ptop = (sumx / (1.0 * nz * mnx)) / 3.0;
+    for (int j = 1; j <= mny; j++) {
+        sumx = 0;
+        for (int i = 1; i <= mnx; i++) {
+            double sumz = 0;
+            for (int k = 1; k <= nz; k++) sumz += rm[IX(S, 1, i, j, k)];
+            sumx += sumz;
+        }
+        const double t = (sumx / (1.0 * nz * mnx)) / 3.0;
+        double *r = prow + 3 * (size_t)(j - 1);
+        r[0] = j;
+        r[1] = t;
+        r[2] = t - ptop;
+    }
+    for (int j = 1; j <= iny; j++) {
+        sumx = 0;
+        for (int i = ia; i <= S->ib; i++) {
+            double sumz = 0;
+            for (int k = 1; k <= nz; k++) sumz += ri[IX(S, 0, i, j, k)];
+            sumx += sumz;
+        }
+        const double t = (sumx / (1.0 * nz * mnx)) / 3.0;
+        double *r = prow + 3 * (size_t)(mny + j - 1);
+        r[0] = j + mny;
+        r[1] = t;
+        r[2] = t - ptop;
+    }
+    for (int i = 1; i <= inx; i++) {
+        double sumy = 0;
+        for (int j = 1; j <= iny; j++) {
+            double sumz = 0;
+            for (int k = 1; k <= nz; k++) sumz += ri[IX(S, 0, i, j, k)];
+            sumy += sumz;
+        }
+        px[2 * (size_t)(i - 1)] = i;
+        px[2 * (size_t)(i - 1) + 1] = (sumy / (1.0 * nz * iny)) / 3.0;
+    }
+    for (int j = 2; j < mny; j++) {
+        double sumz = 0, sumtotalz = 0, allz = 0, alltotalz = 0;
+        for (int k = 2; k < nz; k++) {
+            double sx = 0, stx = 0, allx = 0, alltx = 0;
+            for (int i = 2; i < mnx; i++) {
+#define M_(a, ii, jj, kk) a[IX(S, 1, ii, jj, kk)]
+                const double delux = (M_(ux, i + 1, j, k) - M_(ux, i - 1, j, k)) / 2.0;
+                const double delvy = (M_(uy, i, j + 1, k) - M_(uy, i, j - 1, k)) / 2.0;
+                const double delwz = (M_(uz, i, j, k + 1) - M_(uz, i, j, k - 1)) / 2.0;
+                const double deluy = (M_(ux, i, j + 1, k) - M_(ux, i, j - 1, k)) / 2.0;
+                const double delvx = (M_(uy, i + 1, j, k) - M_(uy, i - 1, j, k)) / 2.0;
+                const double deluz = (M_(ux, i, j, k + 1) - M_(ux, i, j, k - 1)) / 2.0;
+                const double delwx = (M_(uz, i + 1, j, k) - M_(uz, i - 1, j, k)) / 2.0;
+                const double delvz = (M_(uy, i, j, k + 1) - M_(uy, i, j, k - 1)) / 2.0;
+                const double delwy = (M_(uz, i, j + 1, k) - M_(uz, i, j - 1, k)) / 2.0;
+#undef M_
+                sx = pow(delux, 2.0) + pow(delwz, 2.0) + 0.5 * pow((deluz + delwx), 2.0);
+                stx = pow(delux, 2.0) + pow(delvy, 2.0) + pow(delwz, 2.0) + 0.5 * pow((delvx + deluy), 2.0) +
+                      0.5 * pow((deluz + delwx), 2.0) + 0.5 * pow((delvz + delwy), 2.0);
+                allx += sx;
+                alltx += stx;
+            }
+            sumz += sx;
+            sumtotalz += stx;
+            allz += allx;
+            alltotalz += alltx;
+        }
+        double *r = pw + 5 * (size_t)(j - 2);
+        r[0] = j;
+        r[1] = 2.0 * vis * (sumz / (1.0 * (nz - 2) * (mnx - 2)));
+        r[2] = 2.0 * vis * (sumtotalz / (1.0 * (nz - 2) * (mnx - 2)));
+        r[3] = 2.0 * vis * (allz / (1.0 * (nz - 2) * (mnx - 2)));
+        r[4] = 2.0 * vis * (alltotalz / (1.0 * (nz - 2) * (mnx - 2)));
     }
 }
 

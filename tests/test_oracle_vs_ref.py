@@ -41,3 +41,25 @@ def test_oracle_populations_match_reference(name):
             assert bit_equal(got, want), (b, fld, first_mismatch(got, want))
     assert bit_equal(orc.mixing(), mix)
     orc.close()
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_oracle_pressure_power_matches_reference(name):
+    """write_Pressure_Power's numbers (Tmixer.cpp:9866-10027, printed to 17
+    digits by the patched build): the lattice values bit for bit, and the
+    values the reference multiplies by its unit factors too."""
+    case, steps = CASES[name]
+    dump, _, _ = O.run_ref(_binary(name, case), steps, threads=2)
+    ref = dump["pressure"]
+    orc = O.Oracle(case)
+    orc.step(steps)
+    prow, px, pw, (p0, pw0) = orc.pressure_power()
+    orc.close()
+    rows = ref["PressureAlongMixingChannel"]
+    assert bit_equal(rows[:, 0], prow[:, 0]) and bit_equal(rows[:, 1], prow[:, 1])
+    assert bit_equal(rows[:, 2], prow[:, 1] * p0) and bit_equal(rows[:, 3], prow[:, 2] * p0)
+    hor = ref["HorizontalSectionPressure"]
+    assert bit_equal(hor[:, 0], px[:, 0]) and bit_equal(hor[:, 1], px[:, 1]) and bit_equal(hor[:, 2], px[:, 1] * p0)
+    pwr = ref["SpecificPower"]
+    assert bit_equal(pwr[:, 0], pw[:, 0]) and bit_equal(pwr[:, 1], pw[:, 1])
+    assert bit_equal(pwr[:, 2], pw[:, 1] * pw0) and bit_equal(pwr[:, 3], pw[:, 2] * pw0)

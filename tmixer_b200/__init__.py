@@ -112,6 +112,7 @@ def lib() -> ctypes.CDLL:
     L.tmx_mixing.argtypes = [vp, vp, vp]
     L.tmx_mixing_static.argtypes = [vp, vp, vp]
     L.tmx_sums.argtypes = [vp, vp]
+    L.tmx_pressure_power.argtypes = [vp, vp, vp, vp, vp]
     L.tmx_inlet_profile.argtypes = [vp, vp, vp]
     L.tmx_step_timed.argtypes = [vp, ip, P(dp), P(dp), P(dp)]
     L.tmx_counts.argtypes = [vp, P(ctypes.c_longlong)]
@@ -311,6 +312,19 @@ class Solver:
         im = np.empty(3, dtype=np.float64)
         _check(lib().tmx_mixing_static(self._h, rows.ctypes.data, im.ctypes.data))
         return rows, im
+
+    def pressure_power(self):
+        """(pressure rows (mny+iny, 3) {row, p, p - p_top}, inlet
+        cross-sections (inx, 2) {i, p}, power rows (mny-2, 5) {j, section rate,
+        total rate (both as the reference), the same summed over every x},
+        units (P0, Pw0)) as tmx_pressure_power."""
+        s = self.spec
+        prow = np.empty((s.mny + s.iny, 3))
+        px = np.empty((s.inx, 2))
+        pw = np.empty((s.mny - 2, 5))
+        units = np.empty(2)
+        _check(lib().tmx_pressure_power(self._h, prow.ctypes.data, px.ctypes.data, pw.ctypes.data, units.ctypes.data))
+        return prow, px, pw, units
 
     def sums(self) -> np.ndarray:
         out = np.empty(8, dtype=np.float64)

@@ -60,6 +60,7 @@ struct tmx_handle {
     float4* mom[2] = {nullptr, nullptr};  // FP16 form: moments of the nodes that wrote pop[s]
     double* stats = nullptr;
     double* partial = nullptr;
+    double* diag = nullptr;  // pressure / power outputs (allocated on first use)
     std::vector<double> uin1, uin2;
     std::vector<int> class_count;
     int cur = 0;   // population buffer holding the state
@@ -338,6 +339,8 @@ void free_all(tmx_handle* h)
     cudaFree(h->bcls);
     cudaFree(h->stats);
     cudaFree(h->partial);
+    cudaFree(h->diag);
+    h->diag = nullptr;
     h->mac = h->stats = h->partial = nullptr;
     h->bnode = nullptr;
     h->bcls = nullptr;
@@ -839,6 +842,55 @@ int tmx_sums(tmx_handle* h, double out[8])
     out[5] = s[4];
     out[6] = s[5];
     out[7] = (double)h->G.nnodes;
+    return TMX_OK;
+}
+
+int tmx_pressure_power(tmx_handle* h, double* pressure_rows, double* pressure_x, double* power_rows,
+                       double units[2])
+{
+    if (!h || !pressure_rows || !pressure_x || !power_rows || !units) return fail(TMX_E_INVALID, "null argument");
+    if (!h->inited) return fail(TMX_E_STATE, "tmx_pressure_power before tmx_init");
+    TMX_CK(cudaSetDevice(h->device));
+    const Geom& G = h->G;
+    const int nrow = G.mny + G.iny, npow = G.mny - 2, nout = 1 + nrow + G.inx + 4 * npow;
+    if (!h->diag) {
+        cudaError_t e = cudaMalloc((void**)&h->diag, (size_t)nout * sizeof(double));
+        if (e != cudaSuccess) {
+            h->diag = nullptr;
+            cudaGetLastError();
+            return fail(e == cudaErrorMemoryAllocation ? TMX_E_NOMEM : TMX_E_CUDA, "tmx_pressure_power: %s",
+                        cudaGetErrorString(e));
+        }
+        h->bytes += (long long)nout * sizeof(double);
+    }
+    const int items = 1 + nrow + G.inx + npow;
+    tmx::k_pressure_power<<<(items + 127) / 128, 128, 0, h->stream>>>(h->mac, G, h->c.tau, h->diag);
+    TMX_CK(cudaGetLastError());
+    std::vector<double> o((size_t)nout);
+    TMX_CK(cudaMemcpyAsync(o.data(), h->diag, o.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    TMX_CK(cudaStreamSynchronize(h->stream));
+    const double ptop = o[0];
+    for (int r = 0; r < nrow; r++) {
+        pressure_rows[3 * r] = r + 1;  // mixing rows 1..mny, then inlet row j as j + mny
+        pressure_rows[3 * r + 1] = o[1 + r];
+        pressure_rows[3 * r + 2] = o[1 + r] - ptop;
+    }
+    for (int i = 0; i < G.inx; i++) {
+        pressure_x[2 * i] = i + 1;
+        pressure_x[2 * i + 1] = o[1 + nrow + i];
+    }
+    for (int j = 0; j < npow; j++) {
+        power_rows[5 * j] = j + 2;
+        for (int m = 0; m < 4; m++) power_rows[5 * j + 1 + m] = o[1 + nrow + G.inx + 4 * j + m];
+    }
+    // the reference's unit factors (Tmixer.cpp:185-196: LENGTH 0.0008 m, PRESSURE
+    // 101325 Pa, KVISCOSITY 1.004e-6 m^2/s, length = inx), as its macros expand
+    const double tau = h->c.tau, rho0 = h->c.rho0;
+    const double L0 = (0.0008 / (G.inx - 1));
+    const double T0 = ((((2.0 * tau - 1.0) / 6.0) / 0.000001004) * (L0 * L0));
+    const double M0 = ((101325.0 / (rho0 / 3.0)) * (L0 * T0 * T0));
+    units[0] = ((M0) / (L0 * T0 * T0));
+    units[1] = ((L0 * L0) / (T0 * T0 * T0));
     return TMX_OK;
 }
 

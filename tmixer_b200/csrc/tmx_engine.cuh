@@ -1349,12 +1349,19 @@ __device__ __forceinline__ void boundary_lane_lp(const StepPtrs& X, const Geom& 
     }
 }
 
-// Lane fld of boundary node g; buf is the node's 76 values of shared memory.
+// Lane fld of boundary node g in the form's scheme: directions split across
+// the lanes for the interleaved forms (buf: the node's 76 values of shared
+// memory); one field per lane for FP64, whose SoA planes give the direction
+// split no saving and whose larger code then stalls on instruction fetch
+// (65.5 us against 59.6 us for the W=32 faces).
 template <class PR, bool FACES>
 __device__ __forceinline__ void boundary_any(const StepPtrs& X, const Geom& G, const Phys& P, int write_macro, int g,
                                              int cls, int fld, unsigned mask, int lead, typename PR::T* buf)
 {
-    boundary_lane_lp<PR, FACES>(X, G, P, write_macro, g, cls, fld, mask, lead, buf);
+    if constexpr (PR::kOnePass)
+        boundary_lane_lp<PR, FACES>(X, G, P, write_macro, g, cls, fld, mask, lead, buf);
+    else
+        boundary_lane<PR, FACES>(X, G, P, write_macro, g, cls, fld, mask, lead);
 }
 
 // One launch over a node list: thread 4t + fld is lane fld of node t.
@@ -1398,13 +1405,13 @@ __device__ __forceinline__ void bulk_any(const StepPtrs& X, const Geom& G, const
     __global__ void __launch_bounds__(kBoundaryThreads) k_bfaces_##NAME(                                       \
         StepPtrs X, const int* bnode, const unsigned char* bcls, int nb, Geom G, Phys P, int write_macro)       \
     {                                                                                                           \
-        __shared__ PR::T buf[kBoundaryThreads / 4][76];                                                            \
+        __shared__ PR::T buf[PR::kOnePass ? kBoundaryThreads / 4 : 1][76];                                                         \
         boundary_node<PR, true>(X, bnode, bcls, nb, G, P, write_macro, buf);                                    \
     }                                                                                                           \
     __global__ void __launch_bounds__(kBoundaryThreads) k_bedges_##NAME(                                       \
         StepPtrs X, const int* bnode, const unsigned char* bcls, int nb, Geom G, Phys P, int write_macro)       \
     {                                                                                                           \
-        __shared__ PR::T buf[kBoundaryThreads / 4][76];                                                            \
+        __shared__ PR::T buf[PR::kOnePass ? kBoundaryThreads / 4 : 1][76];                                                         \
         boundary_node<PR, false>(X, bnode, bcls, nb, G, P, write_macro, buf);                                   \
     }
 
@@ -1428,7 +1435,7 @@ __device__ __forceinline__ void bulk_any(const StepPtrs& X, const Geom& G, const
         int parity, int write_macro)                                                                            \
     {                                                                                                           \
         const int n = counts[WHICH];                                                                            \
-        __shared__ PR::T buf[kBoundaryThreads / 4][76];                                                            \
+        __shared__ PR::T buf[PR::kOnePass ? kBoundaryThreads / 4 : 1][76];                                                         \
         for (int base = blockIdx.x * blockDim.x; base < 4 * n; base += gridDim.x * blockDim.x) {                \
             const int t = (base + threadIdx.x) >> 2, fld = threadIdx.x & 3;                                     \
             const unsigned mask = __ballot_sync(0xffffffffu, t < n);                                            \

@@ -131,6 +131,91 @@ __global__ void k_mixing_finish(const double* __restrict__ stats, Geom G, double
 }
 
 // ---------------------------------------------------------------------------
+// Pressure and specific power (the numbers of write_Pressure_Power,
+// Tmixer.cpp:9866-10027), one thread per output item, each a sequential sum
+// in the reference's order.  out: [0] the pressure of inlet row iny over the
+// opening (p_top), [1 .. nrow] the row pressures (mixing rows 1..mny, inlet
+// rows 1..iny over x = ia..ib), then inx cross-section pressures of the inlet
+// box, then for each mixing row j = 2..mny-1 four rates: cross-section and
+// total as the reference computes them (its x loop assigns rather than adds,
+// so only column mnx-1 enters the sums over k) and the same two summed over
+// every column.  Pressures are mean density / 3; rates use
+// vis = (2 tau - 1) / 6 and the central differences of the velocity.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double mean_row_rho(const double* __restrict__ rho, const Geom& G, int b, int j, int i0,
+                                               int i1)
+{
+    double sumx = 0.0;
+    for (int i = i0; i <= i1; i++) {
+        double sumz = 0.0;
+        for (int k = 1; k <= G.nz; k++) sumz += rho[node_index(G, b, i, j, k)];
+        sumx += sumz;
+    }
+    return (sumx / (1.0 * G.nz * G.mnx)) / 3.0;
+}
+
+__global__ void k_pressure_power(const double* __restrict__ Mac, Geom G, double tau, double* __restrict__ out)
+{
+    const int nrow = G.mny + G.iny, nitems = 1 + nrow + G.inx + (G.mny - 2);
+    const double* rho = Mac;
+    const double *ux = Mac + G.ps, *uy = Mac + 2 * G.ps, *uz = Mac + 3 * G.ps;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nitems; t += gridDim.x * blockDim.x) {
+        if (t == 0) {
+            out[0] = mean_row_rho(rho, G, 0, G.iny, G.ia, G.ib);
+        } else if (t <= nrow) {
+            const int r = t - 1;
+            out[t] = r < G.mny ? mean_row_rho(rho, G, 1, r + 1, 1, G.mnx)
+                               : mean_row_rho(rho, G, 0, r - G.mny + 1, G.ia, G.ib);
+        } else if (t <= nrow + G.inx) {
+            const int i = t - nrow;
+            double sumy = 0.0;
+            for (int j = 1; j <= G.iny; j++) {
+                double sumz = 0.0;
+                for (int k = 1; k <= G.nz; k++) sumz += rho[node_index(G, 0, i, j, k)];
+                sumy += sumz;
+            }
+            out[t] = (sumy / (1.0 * G.nz * G.iny)) / 3.0;
+        } else {
+            const int j = t - nrow - G.inx + 1;  // 2 .. mny-1
+            const double vis = ((2.0 * tau - 1.0) / 6.0) * (1.0 * 1.0 * 1.0);
+            double sumz = 0.0, sumtotalz = 0.0, allz = 0.0, alltotalz = 0.0;
+            for (int k = 2; k < G.nz; k++) {
+                double sx = 0.0, stx = 0.0, allx = 0.0, alltx = 0.0;
+                for (int i = 2; i < G.mnx; i++) {
+#define TMX_M(a, ii, jj, kk) a[node_index(G, 1, ii, jj, kk)]
+                    const double delux = (TMX_M(ux, i + 1, j, k) - TMX_M(ux, i - 1, j, k)) / 2.0;
+                    const double delvy = (TMX_M(uy, i, j + 1, k) - TMX_M(uy, i, j - 1, k)) / 2.0;
+                    const double delwz = (TMX_M(uz, i, j, k + 1) - TMX_M(uz, i, j, k - 1)) / 2.0;
+                    const double deluy = (TMX_M(ux, i, j + 1, k) - TMX_M(ux, i, j - 1, k)) / 2.0;
+                    const double delvx = (TMX_M(uy, i + 1, j, k) - TMX_M(uy, i - 1, j, k)) / 2.0;
+                    const double deluz = (TMX_M(ux, i, j, k + 1) - TMX_M(ux, i, j, k - 1)) / 2.0;
+                    const double delwx = (TMX_M(uz, i + 1, j, k) - TMX_M(uz, i - 1, j, k)) / 2.0;
+                    const double delvz = (TMX_M(uy, i, j, k + 1) - TMX_M(uy, i, j, k - 1)) / 2.0;
+                    const double delwy = (TMX_M(uz, i, j + 1, k) - TMX_M(uz, i, j - 1, k)) / 2.0;
+#undef TMX_M
+                    const double a = deluz + delwx, bxy = delvx + deluy, c = delvz + delwy;
+                    sx = delux * delux + delwz * delwz + 0.5 * (a * a);
+                    stx = delux * delux + delvy * delvy + delwz * delwz + 0.5 * (bxy * bxy) + 0.5 * (a * a) +
+                          0.5 * (c * c);
+                    allx += sx;
+                    alltx += stx;
+                }
+                sumz += sx;
+                sumtotalz += stx;
+                allz += allx;
+                alltotalz += alltx;
+            }
+            const double n = 1.0 * (G.nz - 2) * (G.mnx - 2);
+            double* o = out + 1 + nrow + G.inx + 4 * (j - 2);
+            o[0] = 2.0 * vis * (sumz / n);
+            o[1] = 2.0 * vis * (sumtotalz / n);
+            o[2] = 2.0 * vis * (allz / n);
+            o[3] = 2.0 * vis * (alltotalz / n);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // FP64 totals: warp-shuffle block reduction, one partial per block
 // ---------------------------------------------------------------------------
 __global__ void k_sums(const double* __restrict__ Mac, Geom G, double* __restrict__ partial)

@@ -76,6 +76,8 @@ __global__ void k_outlet_im_batch(const MixerDesc* D, const int* slots, int n, d
 
 __global__ void k_mixing_rows(const double* __restrict__ Mac, Geom G, double* __restrict__ stats);
 __global__ void k_sums(const double* __restrict__ Mac, Geom G, double* __restrict__ partial);
+// Pressure and specific power of one mixer (layout of out: tmx_kernels.cu).
+__global__ void k_pressure_power(const double* __restrict__ Mac, Geom G, double tau, double* __restrict__ out);
 
 // Fixed scratch of tmx_mixing_static: kMixStaticRows rows of 9 statistics
 // followed by kMixStaticRows finished rows of 7 numbers (512 KiB per device).
