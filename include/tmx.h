@@ -123,6 +123,9 @@ int tmx_sync(tmx_handle *h);
 /* Number of steps completed since tmx_init. */
 long long tmx_steps_done(const tmx_handle *h);
 
+/* The case a handle was created with. */
+int tmx_case_of(const tmx_handle *h, tmx_case *out);
+
 /* Copy one macroscopic field of one box after the last step into host memory
  * (nx*ny*nz doubles).  The arrays rho/ux/uy/uz/grho/hrho/prho (and mrho, mux,
  * ... for the mixing box) of calculate_velocity_density() (Tmixer.cpp:9352-9656),
@@ -177,6 +180,25 @@ int tmx_mixing_static(tmx_handle *h, double *rows_out, double *outlet_im);
  *       pascal and W/kg as it prints them. */
 int tmx_pressure_power(tmx_handle *h, double *pressure_rows, double *pressure_x, double *power_rows,
                        double units[2]);
+
+/* The reference's Tecplot text files, written from the state after the last
+ * step with the reference's own line formats (byte-identical to the
+ * reference's files for the FP64 form):
+ *   TMX_FILE_DOMAIN    Domain_Data: every node of both boxes
+ *                      (write_Domain_Data, Tmixer.cpp:10028-10064)
+ *   TMX_FILE_PVC       Data_P_V_C: the mid-depth plane and five cross-sections
+ *                      (write_Data_P_V_C, :10065-10160); the sections at fixed
+ *                      rows 600, mny-1 and 775-mny are left out where the row
+ *                      is outside its box (the reference reads outside its
+ *                      arrays there)
+ *   TMX_FILE_PRESSURE  Pressure (write_Pressure_Power, :9866-10027)
+ *   TMX_FILE_MIXING    MixingQuality (write_MixingQuality, :10161-10409)
+ * The reference names them Domain_Data_<itr>.dat etc.; path is the caller's. */
+#define TMX_FILE_DOMAIN 0
+#define TMX_FILE_PVC 1
+#define TMX_FILE_PRESSURE 2
+#define TMX_FILE_MIXING 3
+int tmx_write_file(tmx_handle *h, int kind, const char *path);
 
 /* FP64 totals over both boxes after the last step: out[0] = sum rho,
  * out[1..3] = sum cA, cB, cC, out[4] = sum (cA + cB + cC), out[5] = outlet

@@ -201,9 +201,12 @@ def read_ref_pressure(path: str) -> dict:
     return {k: np.array(v, dtype=np.float64) for k, v in zones.items()}
 
 
-def run_ref(binary: str, steps: int, with_pops: bool = False, threads: int | None = None, warmup: int = 0):
+def run_ref(binary: str, steps: int, with_pops: bool = False, threads: int | None = None, warmup: int = 0,
+            writers: str | None = None):
     """Run a reference binary in a scratch directory; return (dump, mixing
-    rows, seconds of the timed loop: the steps after the first ``warmup``)."""
+    rows, seconds of the timed loop: the steps after the first ``warmup``).
+    writers="domain" or "pvc" also collects the reference's Domain_Data (and
+    Data_P_V_C) files as bytes in dump["files"]."""
     env = dict(os.environ)
     if threads:
         env["OMP_NUM_THREADS"] = str(threads)
@@ -211,6 +214,8 @@ def run_ref(binary: str, steps: int, with_pops: bool = False, threads: int | Non
         args = [binary, str(steps), os.path.join(d, "out.bin")] + (["pops"] if with_pops else [])
         if warmup:
             args.append("warmup=%d" % warmup)
+        if writers:
+            args.append("writers=%s" % writers)
         r = subprocess.run(args, cwd=d, env=env, capture_output=True, text=True, check=True)
         secs = None
         for line in r.stderr.splitlines():
@@ -219,4 +224,9 @@ def run_ref(binary: str, steps: int, with_pops: bool = False, threads: int | Non
         dump = read_ref_dump(os.path.join(d, "out.bin"), with_pops)
         mix = read_ref_mixing(os.path.join(d, "MixingQuality_%d.dat" % steps))
         dump["pressure"] = read_ref_pressure(os.path.join(d, "Pressure_%d.dat" % steps))
+        dump["files"] = {}
+        for name in ("Domain_Data_%d.dat" % steps, "Data_P_V_C%d.dat" % steps):
+            if os.path.exists(os.path.join(d, name)):
+                with open(os.path.join(d, name), "rb") as fh:
+                    dump["files"][name.split("%d" % steps)[0].rstrip("_")] = fh.read()
     return dump, mix, secs

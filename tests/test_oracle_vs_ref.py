@@ -13,6 +13,9 @@ from tests.conftest import bit_equal, first_mismatch
 
 CASES = {
     "tiny_ref_pop": (GOLDEN_CASES["tiny_ref"][0], 9),
+    # long and thin: the reference's fixed section rows 600, mny-1 and
+    # 775-mny = 5 of write_Data_P_V_C all lie inside its boxes
+    "pvc_rows": (ref_like(9, 8, 3, 3, 770, umean=0.02), 6),
     "w3_pop": (w_like(3, umean=0.04, tau=0.58, tau_c=0.7, k=0.8, rho=1.2), 25),
     "species_pop": (GOLDEN_CASES["tiny_species"][0], 17),
 }

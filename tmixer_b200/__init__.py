@@ -113,6 +113,8 @@ def lib() -> ctypes.CDLL:
     L.tmx_mixing_static.argtypes = [vp, vp, vp]
     L.tmx_sums.argtypes = [vp, vp]
     L.tmx_pressure_power.argtypes = [vp, vp, vp, vp, vp]
+    L.tmx_write_file.argtypes = [vp, ip, ctypes.c_char_p]
+    L.tmx_case_of.argtypes = [vp, P(_CCase)]
     L.tmx_inlet_profile.argtypes = [vp, vp, vp]
     L.tmx_step_timed.argtypes = [vp, ip, P(dp), P(dp), P(dp)]
     L.tmx_counts.argtypes = [vp, P(ctypes.c_longlong)]
@@ -325,6 +327,13 @@ class Solver:
         units = np.empty(2)
         _check(lib().tmx_pressure_power(self._h, prow.ctypes.data, px.ctypes.data, pw.ctypes.data, units.ctypes.data))
         return prow, px, pw, units
+
+    FILE_KINDS = {"domain": 0, "pvc": 1, "pressure": 2, "mixing": 3}
+
+    def write_file(self, kind: str, path: str) -> None:
+        """One of the reference's Tecplot files ("domain" = Domain_Data,
+        "pvc" = Data_P_V_C, "pressure", "mixing") from the last step."""
+        _check(lib().tmx_write_file(self._h, self.FILE_KINDS[kind], os.fsencode(path)))
 
     def sums(self) -> np.ndarray:
         out = np.empty(8, dtype=np.float64)

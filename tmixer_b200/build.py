@@ -23,7 +23,7 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC"]
 SOURCES = {"tmx_kernels.cu": ["--fmad=false"], "tmx_api.cu": ["--fmad=false"], "tmx_kernels_lp.cu": ["--fmad=true"],
            "tmx_batch.cu": ["--fmad=false"]}
 # host-only C++ sources of the library (no device code)
-CXX_SOURCES = {"tmx_serve.cpp": []}
+CXX_SOURCES = {"tmx_serve.cpp": [], "tmx_writers.cpp": []}
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall"]
 OBJDIR = os.path.join(PKG, "_build")
 

@@ -659,6 +659,13 @@ int tmx_sync(tmx_handle* h)
 
 long long tmx_steps_done(const tmx_handle* h) { return h ? h->steps : -1; }
 
+int tmx_case_of(const tmx_handle* h, tmx_case* out)
+{
+    if (!h || !out) return fail(TMX_E_INVALID, "null argument");
+    *out = h->c;
+    return TMX_OK;
+}
+
 // Copy n = nx*ny*nz doubles of one box from the device (x fastest) into host
 // memory in the reference's [i][j][k] order (k fastest).
 static int box_to_host(tmx_handle* h, int box, const double* dev, double* host_out, std::vector<double>& stage)

@@ -5,7 +5,14 @@
 // the final fields as raw little-endian doubles plus the mixing rows as text.
 //
 //   tmx_run [--case reference | --case w --W 32 --umax 0.05 --tauf 0.56 --tauc 0.6 --k 1e-3 --rho 1]
-//           [--steps N] [--every M] [--out DIR] [--device D]
+//           [--steps N] [--every M] [--out DIR] [--files] [--domain-every D] [--device D]
+//
+// With --files (and --out) it also writes the reference's Tecplot files into
+// DIR at the reference's moments: after step itr+1 for itr % every == 0,
+// Data_P_V_C<itr>.dat, Pressure_<itr>.dat and MixingQuality_<itr>.dat, plus
+// Domain_Data_<itr>.dat when itr % domain-every == 0 (the reference's
+// time_step 1000 and time_domaindata 5000, Tmixer.cpp:147-148, 10476-10486),
+// and Data_P_V_C100.dat after step 101.
 //
 // Output (with --out): DIR/fields.bin = int32 {inx, iny, nz, mnx, mny, ia, ib,
 // steps} then rho, ux, uy, uz, cA, cB, cC of the inlet box and of the mixing
@@ -29,7 +36,8 @@ int main(int argc, char** argv)
 {
     std::string kind = "reference", out;
     int W = 32, device = 0;
-    long long steps = -1, every = 1000;
+    bool files = false;
+    long long steps = -1, every = 1000, domain_every = 5000;
     double umax = 0.05, tauf = 0.56, tauc = 0.6, k = 1e-3, rho = 1.0;
     for (int a = 1; a < argc; a++) {
         auto next = [&](const char* name) -> const char* {
@@ -49,6 +57,8 @@ int main(int argc, char** argv)
         else if (!std::strcmp(argv[a], "--steps")) steps = std::atoll(next("--steps"));
         else if (!std::strcmp(argv[a], "--every")) every = std::atoll(next("--every"));
         else if (!std::strcmp(argv[a], "--out")) out = next("--out");
+        else if (!std::strcmp(argv[a], "--files")) files = true;
+        else if (!std::strcmp(argv[a], "--domain-every")) domain_every = std::atoll(next("--domain-every"));
         else if (!std::strcmp(argv[a], "--device")) device = std::atoi(next("--device"));
         else {
             std::fprintf(stderr, "usage: %s [--case reference|w] [--W n] [--steps n] [--every n] [--out dir]\n",
@@ -74,11 +84,45 @@ int main(int argc, char** argv)
                 c.ia + c.mnx - 1, nodes, steps);
     std::vector<double> rows((size_t)(c.mny + c.iny) * 7);
     double im[3];
+    if (files && out.empty()) {
+        std::fprintf(stderr, "tmx_run: --files needs --out\n");
+        return 2;
+    }
+    if (domain_every <= 0) domain_every = every;
+    // the reference's files after step itr+1 (itr counts from 0)
+    auto write_files = [&](long long itr) -> int {
+        char name[64];
+        const struct {
+            int kind;
+            const char* fmt;
+            bool when;
+        } outs[4] = {{TMX_FILE_PVC, "Data_P_V_C%lld.dat", itr % every == 0 || itr == 100},
+                     {TMX_FILE_PRESSURE, "Pressure_%lld.dat", itr % every == 0},
+                     {TMX_FILE_MIXING, "MixingQuality_%lld.dat", itr % every == 0},
+                     {TMX_FILE_DOMAIN, "Domain_Data_%lld.dat", itr % every == 0 && itr % domain_every == 0}};
+        for (const auto& o : outs) {
+            if (!o.when) continue;
+            std::snprintf(name, sizeof name, o.fmt, itr);
+            if (tmx_write_file(h, o.kind, (out + "/" + name).c_str())) return die("write_file");
+        }
+        return 0;
+    };
     long long done = 0;
     while (done < steps) {
-        const long long n = std::min(every, steps - done);
+        long long n = std::min(every, steps - done);
+        if (files) {  // stop at the next step after which the reference writes
+            const long long itr = done;  // the loop index of the next step
+            long long stop = itr % every == 0 ? itr : (itr / every + 1) * every;
+            if (itr <= 100 && stop > 100) stop = 100;
+            n = std::min(stop - itr + 1, steps - done);
+        }
         if (tmx_step(h, (int)n)) return die("step");
         done += n;
+        if (files) {
+            const long long itr = done - 1;
+            if (itr % every == 0 || itr == 100)
+                if (write_files(itr)) return 1;
+        }
         if (tmx_mixing(h, rows.data(), im)) return die("mixing");
         const double s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         std::printf("step %lld  outlet I_A %.9g I_B %.9g I_C %.9g  %.1f MLUPS\n", done, im[0], im[1], im[2],
