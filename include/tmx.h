@@ -126,6 +126,20 @@ long long tmx_steps_done(const tmx_handle *h);
 /* The case a handle was created with. */
 int tmx_case_of(const tmx_handle *h, tmx_case *out);
 
+/* Checkpoint and restore of a solve's device state (no counterpart in the
+ * reference, which only writes text output): everything the next step reads
+ * (the populations held between steps, the previous step's densities, the
+ * FP16 form's moment records), the macroscopic fields of the last step and
+ * the inlet profiles, behind a header with the case, the form and the step
+ * count.  The buffer is host memory of tmx_checkpoint_size bytes, portable
+ * between handles and batch slots (tmx_batch_checkpoint / tmx_batch_restore)
+ * of the same case and form.  A restored solve continues bit for bit as the
+ * saved one would have; tmx_restore replaces the state of a created handle
+ * (it need not be initialised) and sets its step count. */
+int tmx_checkpoint_size(const tmx_handle *h, long long *bytes);
+int tmx_checkpoint(tmx_handle *h, void *buf, long long bytes);
+int tmx_restore(tmx_handle *h, const void *buf, long long bytes);
+
 /* Copy one macroscopic field of one box after the last step into host memory
  * (nx*ny*nz doubles).  The arrays rho/ux/uy/uz/grho/hrho/prho (and mrho, mux,
  * ... for the mixing box) of calculate_velocity_density() (Tmixer.cpp:9352-9656),
@@ -256,6 +270,14 @@ int tmx_batch_add(tmx_batch *b, const tmx_case *c, int *slot);
 /* Retire a mixer and return its range to the arena; the slot number may be
  * reused by a later tmx_batch_add. */
 int tmx_batch_remove(tmx_batch *b, int slot);
+
+/* Checkpoint one mixer of the batch (format and size as tmx_checkpoint), and
+ * admit a mixer from a checkpoint of case c (taken from a handle or a batch
+ * slot): it continues bit for bit as the saved one would have, from the saved
+ * step count. */
+int tmx_batch_checkpoint_size(const tmx_batch *b, int slot, long long *bytes);
+int tmx_batch_checkpoint(tmx_batch *b, int slot, void *buf, long long bytes);
+int tmx_batch_restore(tmx_batch *b, const tmx_case *c, const void *buf, long long bytes, int *slot);
 
 /* Advance every mixer of the batch by nsteps steps (asynchronous).  With
  * write_macro_last the last step also writes the macroscopic fields that

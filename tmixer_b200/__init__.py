@@ -115,6 +115,9 @@ def lib() -> ctypes.CDLL:
     L.tmx_pressure_power.argtypes = [vp, vp, vp, vp, vp]
     L.tmx_write_file.argtypes = [vp, ip, ctypes.c_char_p]
     L.tmx_case_of.argtypes = [vp, P(_CCase)]
+    L.tmx_checkpoint_size.argtypes = [vp, P(ctypes.c_longlong)]
+    L.tmx_checkpoint.argtypes = [vp, vp, ctypes.c_longlong]
+    L.tmx_restore.argtypes = [vp, vp, ctypes.c_longlong]
     L.tmx_inlet_profile.argtypes = [vp, vp, vp]
     L.tmx_step_timed.argtypes = [vp, ip, P(dp), P(dp), P(dp)]
     L.tmx_counts.argtypes = [vp, P(ctypes.c_longlong)]
@@ -137,6 +140,9 @@ def lib() -> ctypes.CDLL:
     L.tmx_batch_set_shape.argtypes = [vp, ip, ip]
     L.tmx_batch_tune.argtypes = [vp, ip, P(ip), P(ip), P(dp)]
     L.tmx_batch_time_steps.argtypes = [vp, ip, P(dp)]
+    L.tmx_batch_checkpoint_size.argtypes = [vp, ip, P(LL)]
+    L.tmx_batch_checkpoint.argtypes = [vp, ip, vp, LL]
+    L.tmx_batch_restore.argtypes = [vp, P(_CCase), vp, LL, P(ip)]
     L.tmx_batch_destroy.argtypes = [vp]
     L.tmx_batch_destroy.restype = None
     L.tmx_serve.argtypes = [vp, P(_CRequest), ip, P(_CServeOpts), P(_CServed), P(dp)]
@@ -328,6 +334,20 @@ class Solver:
         _check(lib().tmx_pressure_power(self._h, prow.ctypes.data, px.ctypes.data, pw.ctypes.data, units.ctypes.data))
         return prow, px, pw, units
 
+    def checkpoint(self) -> bytes:
+        """The solve's state (tmx_checkpoint) as bytes."""
+        n = ctypes.c_longlong()
+        _check(lib().tmx_checkpoint_size(self._h, ctypes.byref(n)))
+        buf = ctypes.create_string_buffer(n.value)
+        _check(lib().tmx_checkpoint(self._h, buf, n.value))
+        return buf.raw
+
+    def restore(self, data: bytes) -> "Solver":
+        """Replace the state with a checkpoint of the same case and form."""
+        buf = ctypes.create_string_buffer(bytes(data), len(data))
+        _check(lib().tmx_restore(self._h, buf, len(data)))
+        return self
+
     FILE_KINDS = {"domain": 0, "pvc": 1, "pressure": 2, "mixing": 3}
 
     def write_file(self, kind: str, path: str) -> None:
@@ -396,6 +416,22 @@ class Batch:
     def remove(self, slot: int) -> None:
         _check(lib().tmx_batch_remove(self._b, int(slot)))
         self.specs.pop(int(slot), None)
+
+    def checkpoint(self, slot: int) -> bytes:
+        n = ctypes.c_longlong()
+        _check(lib().tmx_batch_checkpoint_size(self._b, int(slot), ctypes.byref(n)))
+        buf = ctypes.create_string_buffer(n.value)
+        _check(lib().tmx_batch_checkpoint(self._b, int(slot), buf, n.value))
+        return buf.raw
+
+    def restore(self, spec: CaseSpec, data: bytes) -> int:
+        """Admit a mixer from a checkpoint of ``spec``; returns its slot."""
+        c = spec.to_c()
+        buf = ctypes.create_string_buffer(bytes(data), len(data))
+        slot = ctypes.c_int()
+        _check(lib().tmx_batch_restore(self._b, ctypes.byref(c), buf, len(data), ctypes.byref(slot)))
+        self.specs[slot.value] = spec
+        return slot.value
 
     def step(self, n: int = 1, write_macro: bool = True) -> "Batch":
         _check(lib().tmx_batch_step(self._b, int(n), 1 if write_macro else 0))

@@ -456,6 +456,24 @@ int check_case(const tmx_case& cc)
     return TMX_OK;
 }
 
+int checkpoint_check(const void* buf, long long size, const tmx_case& c, const Geom& G)
+{
+    if (size < (long long)sizeof(CheckpointHeader)) return fail(TMX_E_INVALID, "checkpoint too small");
+    CheckpointHeader hd;
+    std::memcpy(&hd, buf, sizeof hd);
+    if (std::memcmp(hd.magic, "TMXCKPT1", 8) != 0) return fail(TMX_E_INVALID, "not a checkpoint");
+    if (hd.abi != TMX_ABI_VERSION) return fail(TMX_E_INVALID, "checkpoint of ABI %d, library %d", hd.abi, TMX_ABI_VERSION);
+    if (hd.precision != c.precision)
+        return fail(TMX_E_INVALID, "checkpoint of precision %d, target %d", hd.precision, c.precision);
+    if (std::memcmp(&hd.c, &c, sizeof c) != 0) return fail(TMX_E_INVALID, "checkpoint of a different case");
+    long long b[5];
+    checkpoint_sections(G, c.precision, b);
+    if (hd.ps != G.ps || std::memcmp(hd.bytes, b, sizeof b) != 0 || size != checkpoint_total(b))
+        return fail(TMX_E_INVALID, "checkpoint sizes do not match the case");
+    if (hd.steps < 0) return fail(TMX_E_INVALID, "checkpoint with a negative step count");
+    return TMX_OK;
+}
+
 }  // namespace tmx_host
 
 extern "C" {
@@ -658,6 +676,80 @@ int tmx_sync(tmx_handle* h)
 }
 
 long long tmx_steps_done(const tmx_handle* h) { return h ? h->steps : -1; }
+
+int tmx_checkpoint_size(const tmx_handle* h, long long* bytes)
+{
+    if (!h || !bytes) return fail(TMX_E_INVALID, "null argument");
+    long long b[5];
+    checkpoint_sections(h->G, h->c.precision, b);
+    *bytes = checkpoint_total(b);
+    return TMX_OK;
+}
+
+int tmx_checkpoint(tmx_handle* h, void* buf, long long size)
+{
+    if (!h || !buf) return fail(TMX_E_INVALID, "null argument");
+    if (!h->inited) return fail(TMX_E_STATE, "tmx_checkpoint before tmx_init");
+    long long b[5];
+    checkpoint_sections(h->G, h->c.precision, b);
+    if (size != checkpoint_total(b)) return fail(TMX_E_INVALID, "checkpoint buffer of %lld bytes, %lld needed", size,
+                                                 checkpoint_total(b));
+    TMX_CK(cudaSetDevice(h->device));
+    TMX_CK(cudaStreamSynchronize(h->stream));
+    CheckpointHeader hd{};
+    std::memcpy(hd.magic, "TMXCKPT1", 8);
+    hd.abi = TMX_ABI_VERSION;
+    hd.precision = h->c.precision;
+    hd.c = h->c;
+    hd.steps = h->steps;
+    hd.ps = h->G.ps;
+    std::memcpy(hd.bytes, b, sizeof b);
+    char* p = (char*)buf;
+    std::memcpy(p, &hd, sizeof hd);
+    p += sizeof hd;
+    const void* src[4] = {h->pop[h->cur], h->rho[h->cur], h->mom[h->cur], h->mac};
+    for (int k = 0; k < 4; k++) {
+        if (b[k]) TMX_CK(cudaMemcpy(p, src[k], (size_t)b[k], cudaMemcpyDeviceToHost));
+        p += b[k];
+    }
+    std::memcpy(p, h->uin1.data(), (size_t)b[4] / 2);
+    std::memcpy(p + b[4] / 2, h->uin2.data(), (size_t)b[4] / 2);
+    return TMX_OK;
+}
+
+int tmx_restore(tmx_handle* h, const void* buf, long long size)
+{
+    if (!h || !buf) return fail(TMX_E_INVALID, "null argument");
+    int rc = checkpoint_check(buf, size, h->c, h->G);
+    if (rc) return rc;
+    TMX_CK(cudaSetDevice(h->device));
+    TMX_CK(cudaStreamSynchronize(h->stream));
+    CheckpointHeader hd;
+    std::memcpy(&hd, buf, sizeof hd);
+    const char* p = (const char*)buf + sizeof hd;
+    // the state goes into buffer set 0, which the next step then reads
+    void* dst[4] = {h->pop[0], h->rho[0], h->mom[0], h->mac};
+    for (int k = 0; k < 4; k++) {
+        if (hd.bytes[k]) TMX_CK(cudaMemcpy(dst[k], p, (size_t)hd.bytes[k], cudaMemcpyHostToDevice));
+        p += hd.bytes[k];
+    }
+    const size_t nu = (size_t)(h->G.iny + 3) * (h->G.nz + 3);
+    h->uin1.assign((const double*)p, (const double*)p + nu);
+    h->uin2.assign((const double*)p + nu, (const double*)p + 2 * nu);
+    if (h->tbytes == 8) {
+        TMX_CK(cudaMemcpy(h->uin_d[0], h->uin1.data(), nu * 8, cudaMemcpyHostToDevice));
+        TMX_CK(cudaMemcpy(h->uin_d[1], h->uin2.data(), nu * 8, cudaMemcpyHostToDevice));
+    } else {
+        std::vector<float> a(h->uin1.begin(), h->uin1.end()), c(h->uin2.begin(), h->uin2.end());
+        TMX_CK(cudaMemcpy(h->uin_d[0], a.data(), nu * 4, cudaMemcpyHostToDevice));
+        TMX_CK(cudaMemcpy(h->uin_d[1], c.data(), nu * 4, cudaMemcpyHostToDevice));
+    }
+    h->cur = 0;
+    h->rcur = 0;
+    h->steps = hd.steps;
+    h->inited = true;
+    return TMX_OK;
+}
 
 int tmx_case_of(const tmx_handle* h, tmx_case* out)
 {

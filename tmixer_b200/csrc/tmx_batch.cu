@@ -453,7 +453,43 @@ int tmx_batch_create(int precision, long long budget_bytes, int device, tmx_batc
     return TMX_OK;
 }
 
-int tmx_batch_add(tmx_batch* b, const tmx_case* c, int* slot)
+}  // extern "C"
+
+namespace {
+
+// Restore a checkpoint (format in tmx_host.h) into a freshly carved slot: the
+// state goes into buffer set 0 with parity0 = the batch's parity, so the
+// next batch step reads it.
+int restore_slot(tmx_batch* b, Slot& s, const void* buf, long long size)
+{
+    int rc = checkpoint_check(buf, size, s.c, s.G);
+    if (rc) return rc;
+    CheckpointHeader hd;
+    std::memcpy(&hd, buf, sizeof hd);
+    const char* p = (const char*)buf + sizeof hd;
+    void* dst[4] = {s.pop[0], s.rho[0], s.mom[0], s.mac};
+    for (int k = 0; k < 4; k++) {
+        if (hd.bytes[k]) TMX_CK(cudaMemcpyAsync(dst[k], p, (size_t)hd.bytes[k], cudaMemcpyHostToDevice, b->stream));
+        p += hd.bytes[k];
+    }
+    const size_t nu = (size_t)(s.G.iny + 3) * (s.G.nz + 3);
+    const double* u = (const double*)p;
+    if (b->K->tbytes == 8) {
+        TMX_CK(cudaMemcpyAsync(s.uin[0], u, nu * 8, cudaMemcpyHostToDevice, b->stream));
+        TMX_CK(cudaMemcpyAsync(s.uin[1], u + nu, nu * 8, cudaMemcpyHostToDevice, b->stream));
+    } else {
+        std::vector<float> a(u, u + nu), c(u + nu, u + 2 * nu);
+        TMX_CK(cudaMemcpyAsync(s.uin[0], a.data(), nu * 4, cudaMemcpyHostToDevice, b->stream));
+        TMX_CK(cudaMemcpyAsync(s.uin[1], c.data(), nu * 4, cudaMemcpyHostToDevice, b->stream));
+    }
+    TMX_CK(cudaStreamSynchronize(b->stream));
+    s.parity0 = b->parity;
+    s.steps = hd.steps;
+    return TMX_OK;
+}
+
+// Carve a slot for case c and either start it (buf == nullptr) or restore it.
+int admit(tmx_batch* b, const tmx_case* c, const void* buf, long long size, int* slot)
 {
     if (!b || !c || !slot) return fail(TMX_E_INVALID, "null argument");
     *slot = -1;
@@ -506,7 +542,7 @@ int tmx_batch_add(tmx_batch* b, const tmx_case* c, int* slot)
         b->slots.emplace_back();
     }
     b->slots[m] = std::move(s);
-    rc = init_slot(b, b->slots[m]);
+    rc = buf ? restore_slot(b, b->slots[m], buf, size) : init_slot(b, b->slots[m]);
     if (rc) {
         b->arena.release(off, cv.total);
         b->slots[m] = Slot();
@@ -514,6 +550,63 @@ int tmx_batch_add(tmx_batch* b, const tmx_case* c, int* slot)
     }
     b->dirty = true;
     *slot = m;
+    return TMX_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tmx_batch_add(tmx_batch* b, const tmx_case* c, int* slot) { return admit(b, c, nullptr, 0, slot); }
+
+int tmx_batch_restore(tmx_batch* b, const tmx_case* c, const void* buf, long long bytes, int* slot)
+{
+    if (!buf) return fail(TMX_E_INVALID, "null checkpoint");
+    return admit(b, c, buf, bytes, slot);
+}
+
+int tmx_batch_checkpoint(tmx_batch* b, int slot, void* buf, long long bytes)
+{
+    if (!b || !buf) return fail(TMX_E_INVALID, "null argument");
+    if (!valid_slot(b, slot)) return fail(TMX_E_INVALID, "slot %d is not in the batch", slot);
+    const Slot& s = b->slots[slot];
+    long long sec[5];
+    checkpoint_sections(s.G, b->precision, sec);
+    if (bytes != checkpoint_total(sec))
+        return fail(TMX_E_INVALID, "checkpoint buffer of %lld bytes, %lld needed", bytes, checkpoint_total(sec));
+    TMX_CK(cudaSetDevice(b->device));
+    TMX_CK(cudaStreamSynchronize(b->stream));
+    CheckpointHeader hd{};
+    std::memcpy(hd.magic, "TMXCKPT1", 8);
+    hd.abi = TMX_ABI_VERSION;
+    hd.precision = b->precision;
+    hd.c = s.c;
+    hd.steps = s.steps;
+    hd.ps = s.G.ps;
+    std::memcpy(hd.bytes, sec, sizeof sec);
+    char* p = (char*)buf;
+    std::memcpy(p, &hd, sizeof hd);
+    p += sizeof hd;
+    const int q = b->parity ^ s.parity0;  // the buffer set the next step reads
+    const void* src[4] = {s.pop[q], s.rho[q], s.mom[q], s.mac};
+    for (int k = 0; k < 4; k++) {
+        if (sec[k]) TMX_CK(cudaMemcpy(p, src[k], (size_t)sec[k], cudaMemcpyDeviceToHost));
+        p += sec[k];
+    }
+    std::vector<double> u1, u2;
+    cached_inlet(s.c, u1, u2);
+    std::memcpy(p, u1.data(), u1.size() * 8);
+    std::memcpy(p + u1.size() * 8, u2.data(), u2.size() * 8);
+    return TMX_OK;
+}
+
+int tmx_batch_checkpoint_size(const tmx_batch* b, int slot, long long* bytes)
+{
+    if (!b || !bytes) return fail(TMX_E_INVALID, "null argument");
+    if (!valid_slot(b, slot)) return fail(TMX_E_INVALID, "slot %d is not in the batch", slot);
+    long long sec[5];
+    checkpoint_sections(b->slots[slot].G, b->precision, sec);
+    *bytes = checkpoint_total(sec);
     return TMX_OK;
 }
 

@@ -63,4 +63,35 @@ void inlet_series(int iny, int nz, std::vector<double>& raw, double& average);
 void inlet_scale(const tmx_case& c, const std::vector<double>& raw, double average, std::vector<double>& U1,
                  std::vector<double>& U2);
 
+// Checkpoint layout (tmx_checkpoint, tmx_batch_checkpoint): this header, then
+// the sections in the order of `bytes`: the population buffer the next step
+// reads (76 planes of ps values of the storage type), the previous step's
+// densities (4 planes, arithmetic type), the FP16 form's moment records
+// (2 float4 per node, or nothing), the macroscopic fields (7 FP64 planes) and
+// the two inlet profiles ((iny+3)(nz+3) FP64 values each).
+struct CheckpointHeader {
+    char magic[8];  // "TMXCKPT1"
+    int abi;
+    int precision;
+    tmx_case c;
+    long long steps;
+    long long ps;
+    long long bytes[5];
+};
+inline void checkpoint_sections(const Geom& G, int precision, long long bytes[5])
+{
+    const StepKernels& K = kForms[precision];
+    bytes[0] = 76LL * G.ps * K.sbytes;
+    bytes[1] = 4LL * G.ps * K.tbytes;
+    bytes[2] = K.moments ? 2LL * G.ps * 16 : 0;
+    bytes[3] = 7LL * G.ps * 8;
+    bytes[4] = 2LL * (G.iny + 3) * (G.nz + 3) * 8;
+}
+inline long long checkpoint_total(const long long bytes[5])
+{
+    return (long long)sizeof(CheckpointHeader) + bytes[0] + bytes[1] + bytes[2] + bytes[3] + bytes[4];
+}
+// Check a checkpoint against a case; TMX_OK or TMX_E_INVALID with a message.
+int checkpoint_check(const void* buf, long long size, const tmx_case& c, const Geom& G);
+
 }  // namespace tmx_host
