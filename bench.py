@@ -323,6 +323,21 @@ def run_ours(args, dist: Dist) -> dict | None:
            "steps": e2e_steps, "seconds": e2e_s,
            "what": "create + init + %d steps + mixing index every 100 steps + all fields to host" % e2e_steps}
 
+    # the reference's own case (401x51x51 + 101x750x51, 4.9M nodes), plain FP64
+    refcase = None
+    if not args.no_forms:
+        rs = T.Solver(T.reference_case(), device=dist.local_rank).init()
+        rs.step(args.warmup)
+        rs.sync()
+        n_ref = min(args.steps, 300)
+        ms_ref = dist.max(rs.time_steps(n_ref), dev)
+        nodes_ref = rs.spec.nodes()
+        rs.close()
+        refcase = {"workload": "the reference's own case (inlet 401x51x51 + mixing 101x750x51), plain FP64",
+                   "fluid_nodes": nodes_ref, "steps": n_ref, "ms_per_step": ms_ref / n_ref,
+                   "mlups": dist.world * nodes_ref * n_ref / (ms_ref * 1e-3) / 1e6,
+                   "hbm_frac_step": nodes_ref * FORM_BYTES["fp64"] / (ms_ref / n_ref * 1e-3) / 1e9 / peaks["hbm_gbs"]}
+
     batched = served = None
     if not args.no_batched:
         fp64 = forms.get("fp64", {}).get("mlups") or (value if args.form == "fp64" else None)
@@ -345,7 +360,8 @@ def run_ours(args, dist: Dist) -> dict | None:
             "data": "synthetic",
             "config": config_dict(spec, form_text[args.form], dist.world),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
-            "gpu_launches": 3 * args.steps, "forms": forms, "batched": batched, "served": served}
+            "gpu_launches": 3 * args.steps, "forms": forms, "reference_case": refcase, "batched": batched,
+            "served": served}
 
 
 # ---------------------------------------------------------------------------
