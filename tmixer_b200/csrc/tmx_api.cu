@@ -81,9 +81,9 @@ struct tmx_handle {
 };
 
 const StepKernels tmx_host::kForms[3] = {
-    {tmx::k_init_f64, tmx::k_bulk_f64, tmx::k_bfaces_f64, tmx::k_bedges_f64, 8, 8, false},
-    {tmx::k_init_f32, tmx::k_bulk_f32, tmx::k_bfaces_f32, tmx::k_bedges_f32, 4, 4, false},
-    {tmx::k_init_f16, tmx::k_bulk_f16, tmx::k_bfaces_f16, tmx::k_bedges_f16, 2, 4, true},
+    {tmx::k_init_f64, tmx::k_bulk_f64, tmx::k_bfaces_f64, tmx::k_bedges_f64, 8, 8, false, true},
+    {tmx::k_init_f32, tmx::k_bulk_f32, tmx::k_bfaces_f32, tmx::k_bedges_f32, 4, 4, false, false},
+    {tmx::k_init_f16, tmx::k_bulk_f16, tmx::k_bfaces_f16, tmx::k_bedges_f16, 2, 4, true, false},
 };
 
 namespace tmx_host {
@@ -383,11 +383,23 @@ int enqueue_step(tmx_handle* h, int cur, int write_macro, cudaEvent_t* ev)
         TMX_CK(cudaEventRecord(ev[3], h->aux));
     }
     TMX_CK(cudaEventRecord(h->join, h->aux));
+    // FP64: the bulk kernel follows the two boundary kernels.  Its blocks and
+    // theirs (about 120 registers each) cannot share an SM, so running them
+    // side by side only stretched the bulk launch (step 204 us side by side,
+    // 202 us in order at W=32).  The reduced-precision boundary kernels (64
+    // registers) do overlap the bulk kernel (FP16 step 75 us side by side,
+    // 85 us in order).
+    if (h->K->serial) {
+        TMX_CK(cudaStreamWaitEvent(h->stream, h->join, 0));
+        TMX_CK(cudaStreamWaitEvent(h->stream, h->join2, 0));
+    }
     if (ev) TMX_CK(cudaEventRecord(ev[0], h->stream));
     h->K->bulk<<<h->bulk_blocks, 256, 0, h->stream>>>(X, G, h->P, write_macro);
     if (ev) TMX_CK(cudaEventRecord(ev[1], h->stream));
-    TMX_CK(cudaStreamWaitEvent(h->stream, h->join, 0));
-    TMX_CK(cudaStreamWaitEvent(h->stream, h->join2, 0));
+    if (!h->K->serial) {
+        TMX_CK(cudaStreamWaitEvent(h->stream, h->join, 0));
+        TMX_CK(cudaStreamWaitEvent(h->stream, h->join2, 0));
+    }
     TMX_CK(cudaGetLastError());
     return TMX_OK;
 }

@@ -325,11 +325,19 @@ int enqueue(tmx_batch* b, int parity, int write_macro)
     b->B->edges<<<b->grid_edges, bt, 0, b->aux2>>>(b->d_desc, b->d_edges, b->d_counts, parity, write_macro);
     TMX_CK(cudaEventRecord(b->join2, b->aux2));
     TMX_CK(cudaEventRecord(b->join, b->aux));
+    // in order for FP64, side by side for the reduced-precision forms (as the
+    // single-mixer step; StepKernels::serial)
+    if (b->K->serial) {
+        TMX_CK(cudaStreamWaitEvent(b->stream, b->join, 0));
+        TMX_CK(cudaStreamWaitEvent(b->stream, b->join2, 0));
+    }
     b->B->bulk[b->variant]<<<b->grid_bulk[b->variant], kBulkThreads[b->variant], 0, b->stream>>>(
         b->d_desc, b->d_blocks, b->d_counts, parity, write_macro);
     TMX_CK(cudaGetLastError());
-    TMX_CK(cudaStreamWaitEvent(b->stream, b->join, 0));
-    TMX_CK(cudaStreamWaitEvent(b->stream, b->join2, 0));
+    if (!b->K->serial) {
+        TMX_CK(cudaStreamWaitEvent(b->stream, b->join, 0));
+        TMX_CK(cudaStreamWaitEvent(b->stream, b->join2, 0));
+    }
     return TMX_OK;
 }
 

@@ -37,6 +37,7 @@ struct StepKernels {
     void (*edges)(tmx::StepPtrs, const int*, const unsigned char*, int, Geom, Phys, int);
     int sbytes, tbytes;
     bool moments;  // the form stores per-node FP32 moments next to the populations
+    bool serial;   // the bulk kernel runs after the boundary kernels, not beside them
 };
 extern const StepKernels kForms[3];
 
