@@ -298,6 +298,11 @@ long long tmx_batch_slot_steps(const tmx_batch *b, int slot);
  * macroscopic fields of the last step that wrote them; waits for the result. */
 int tmx_batch_outlet_im(tmx_batch *b, const int *slots, int n, double *im_out);
 
+/* Health of n mixers: bad[e] = 1 if mixer slots[e] has a non-finite density,
+ * velocity or concentration in the macroscopic fields of the last step that
+ * wrote them (checked on the device over all its nodes), else 0. */
+int tmx_batch_health(tmx_batch *b, const int *slots, int n, int *bad);
+
 /* One macroscopic field of one box of one mixer, as tmx_fields. */
 int tmx_batch_fields(tmx_batch *b, int slot, int box, int field, double *host_out);
 
@@ -343,7 +348,8 @@ typedef struct tmx_request {
 } tmx_request;
 
 typedef struct tmx_served {
-    int status;         /* 0 converged, 1 stopped at max_steps, TMX_E_NOMEM larger than the whole budget */
+    int status;         /* 0 converged, 1 stopped at max_steps, TMX_E_NOMEM larger than the whole budget,
+                           TMX_E_NONFINITE retired because its state became non-finite */
     int slot;           /* batch slot it ran in */
     long long steps;    /* steps taken */
     double admitted;    /* seconds after the start */
@@ -376,6 +382,9 @@ typedef struct tmx_serve_ops {
     int (*outlet_im)(void *ctx, const int *slots, int n, double *im);
     double (*now)(void *ctx);
     void (*wait_until)(void *ctx, double t);
+    /* optional (may be NULL): bad[e] = 1 for a mixer whose state is no longer
+     * finite; such a mixer is retired at once with status TMX_E_NONFINITE */
+    int (*health)(void *ctx, const int *slots, int n, int *bad);
 } tmx_serve_ops;
 
 int tmx_serve_with(const tmx_serve_ops *ops, const tmx_request *reqs, int n, const tmx_serve_opts *opts,

@@ -4,6 +4,7 @@ index, bit for bit), whether its neighbours arrive before, with or after it
 and whether the budget lets all of them in at once or only two."""
 import dataclasses
 
+import numpy as np
 import pytest
 
 import tmixer_b200 as T
@@ -54,3 +55,26 @@ def test_served_outlet_index_matches_solver(gpu):
         s.step(r["steps"])
         _, im = s.mixing()
     assert list(im) == r["outlet_im"]
+
+
+def test_health_flags_non_finite_mixers(gpu):
+    """A mixer restored from a checkpoint whose populations were overwritten
+    with NaN is flagged by the device health check after a step; its
+    neighbour in the batch is not, and keeps its exact result."""
+    healthy, sick = _requests()[0].spec, _requests()[1].spec
+    with T.Solver(sick) as s:
+        s.init()
+        s.step(5)
+        ck = bytearray(s.checkpoint())
+    ck[1000:1256] = b"\x7e" * 256  # FP16 0x7E7E: NaN
+    with T.Batch(T.TMX_FP16, budget=1 << 27) as B:
+        a = B.add(healthy)
+        b = B.restore(sick, bytes(ck))
+        B.step(2)
+        assert B.health([a, b]) == [0, 1]
+        B.step(3)
+        with T.Solver(healthy) as s:
+            s.init()
+            s.step(5)
+            want = s.field(1, "cA")
+        assert np.array_equal(B.field(a, 1, "cA"), want)

@@ -169,3 +169,23 @@ def test_undefined_index_never_converges():
     eng = FakeEngine(capacity=10**9)
     res, _ = T.serve_with(eng, [T.Request(spec(4, -1.0), 0.0, 2000, 500, 1e-6)], check_every=CHECK)
     assert (res[0]["status"], res[0]["steps"]) == ("max_steps", 2000)
+
+
+class SickEngine(FakeEngine):
+    """A fake engine whose mixers of tau == 777 turn non-finite after 300
+    steps."""
+
+    def health(self, slots):
+        return [int(self.slots[s]["spec"].rateconst == 777.0 and self.slots[s]["steps"] >= 300) for s in slots]
+
+
+def test_non_finite_mixer_retired_and_backfilled():
+    s = spec(4, 400.0)
+    reqs = [T.Request(spec(4, 777.0), 0.0, 50000, 500, 1e-6), T.Request(spec(4, 400.0), 0.0, 50000, 500, 1e-6)]
+    eng = SickEngine(capacity=s.nodes() * 100 + 10)  # one mixer at a time
+    res, summ = T.serve_with(eng, reqs, check_every=CHECK)
+    assert (res[0]["status"], res[0]["steps"]) == ("non-finite", 300)
+    assert res[1]["status"] == "converged"
+    assert res[1]["admitted"] == res[0]["finished"]  # back-filled at once
+    # a diverged solve has no time to solution
+    assert summ["p99_s"] == res[1]["time_to_solution"]

@@ -75,11 +75,14 @@ _OUTLET = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.
                            ctypes.POINTER(ctypes.c_double))
 _NOW = ctypes.CFUNCTYPE(ctypes.c_double, ctypes.c_void_p)
 _WAIT = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_double)
+_HEALTH = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.c_int,
+                           ctypes.POINTER(ctypes.c_int))
 
 
 class _CServeOps(ctypes.Structure):
     _fields_ = [("ctx", ctypes.c_void_p), ("footprint", _FOOTPRINT), ("capacity", _CAPACITY), ("add", _ADD),
-                ("remove", _REMOVE), ("step", _STEP), ("outlet_im", _OUTLET), ("now", _NOW), ("wait_until", _WAIT)]
+                ("remove", _REMOVE), ("step", _STEP), ("outlet_im", _OUTLET), ("now", _NOW), ("wait_until", _WAIT),
+                ("health", _HEALTH)]
 
 
 _lib = None
@@ -136,6 +139,7 @@ def lib() -> ctypes.CDLL:
     L.tmx_batch_slot_steps.restype = LL
     L.tmx_batch_outlet_im.argtypes = [vp, P(ip), ip, vp]
     L.tmx_batch_fields.argtypes = [vp, ip, ip, ip, vp]
+    L.tmx_batch_health.argtypes = [vp, P(ip), ip, P(ip)]
     L.tmx_batch_info.argtypes = [vp, P(LL)]
     L.tmx_batch_set_shape.argtypes = [vp, ip, ip]
     L.tmx_batch_tune.argtypes = [vp, ip, P(ip), P(ip), P(dp)]
@@ -459,6 +463,15 @@ class Batch:
         _check(lib().tmx_batch_outlet_im(self._b, arr, len(slots), out.ctypes.data))
         return out
 
+    def health(self, slots=None) -> list:
+        """1 for every mixer whose last macroscopic fields hold a non-finite
+        value, else 0 (tmx_batch_health)."""
+        slots = self.slots() if slots is None else list(slots)
+        arr = (ctypes.c_int * max(1, len(slots)))(*slots)
+        bad = (ctypes.c_int * max(1, len(slots)))()
+        _check(lib().tmx_batch_health(self._b, arr, len(slots), bad))
+        return list(bad[:len(slots)])
+
     def field(self, slot: int, box: int, name: str) -> np.ndarray:
         s = self.specs[int(slot)]
         shape = (s.inx, s.iny, s.nz) if box == 0 else (s.mnx, s.mny, s.nz)
@@ -519,7 +532,7 @@ class Request:
                          float(self.tol))
 
 
-SERVE_STATUS = {0: "converged", 1: "max_steps", -2: "too large for the budget"}
+SERVE_STATUS = {0: "converged", 1: "max_steps", -2: "too large for the budget", -5: "non-finite"}
 
 
 def _serve_out(reqs, res, summ):
@@ -548,7 +561,8 @@ def serve_with(engine, requests, check_every: int = 100, max_active: int = 0):
     """Run the same request loop (tmx_serve_with) over a Python engine object
     with methods footprint(spec), capacity(), add(spec) -> slot or None when it
     does not fit now, remove(slot), step(n), outlet_im(slots) -> (n, 3),
-    now(), wait_until(t).  For tests of the scheduler without a GPU."""
+    now(), wait_until(t), and optionally health(slots) -> list of 0/1 (1: the
+    mixer's state is non-finite).  For tests of the scheduler without a GPU."""
     reqs = list(requests)
     errors = []
 
@@ -587,9 +601,16 @@ def serve_with(engine, requests, check_every: int = 100, max_active: int = 0):
                 out[3 * i + s] = float(v[i, s])
         return 0
 
+    def health(_, slots, n, bad):
+        v = engine.health([slots[i] for i in range(n)])
+        for i in range(n):
+            bad[i] = int(v[i])
+        return 0
+
     cbs = [_FOOTPRINT(guard(fp)), _CAPACITY(guard(lambda _: int(engine.capacity()), 0)), _ADD(guard(add)),
            _REMOVE(guard(rem)), _STEP(guard(step)), _OUTLET(guard(im)), _NOW(guard(lambda _: float(engine.now()), 0.0)),
-           _WAIT(guard(lambda _, t: engine.wait_until(float(t)), None))]
+           _WAIT(guard(lambda _, t: engine.wait_until(float(t)), None)),
+           _HEALTH(guard(health)) if hasattr(engine, "health") else _HEALTH()]
     ops = _CServeOps(None, *cbs)
     arr = (_CRequest * max(1, len(reqs)))(*[q.to_c() for q in reqs])
     res = (_CServed * max(1, len(reqs)))()

@@ -192,6 +192,8 @@ struct tmx_batch {
     int* d_counts = nullptr;
     int* d_slots = nullptr;
     double* d_im = nullptr;
+    int* d_flags = nullptr;  // per-slot health flags (tmx_batch_health)
+    int cap_flags = 0;
     int cap_im = 0;
     long long table_bytes = 0;
     bool dirty = true;
@@ -706,6 +708,36 @@ int tmx_batch_outlet_im(tmx_batch* b, const int* slots, int n, double* im_out)
     return TMX_OK;
 }
 
+int tmx_batch_health(tmx_batch* b, const int* slots, int n, int* bad)
+{
+    if (!b || (n > 0 && (!slots || !bad))) return fail(TMX_E_INVALID, "null argument");
+    if (n <= 0) return TMX_OK;
+    for (int e = 0; e < n; e++)
+        if (!valid_slot(b, slots[e])) return fail(TMX_E_INVALID, "slot %d is not in the batch", slots[e]);
+    TMX_CK(cudaSetDevice(b->device));
+    if (b->dirty) {
+        int rc = rebuild(b);
+        if (rc) return rc;
+    }
+    const int ns = (int)b->slots.size();
+    if (ns > b->cap_flags) {
+        TMX_CK(cudaStreamSynchronize(b->stream));
+        cudaFree(b->d_flags);
+        b->d_flags = nullptr;
+        b->cap_flags = 0;
+        TMX_CK(cudaMalloc((void**)&b->d_flags, (size_t)std::max(ns, 64) * sizeof(int)));
+        b->cap_flags = std::max(ns, 64);
+    }
+    TMX_CK(cudaMemsetAsync(b->d_flags, 0, (size_t)ns * sizeof(int), b->stream));
+    tmx::k_nonfinite_batch<<<b->sms * 4, 256, 0, b->stream>>>(b->d_desc, b->d_blocks, b->d_counts, b->d_flags);
+    TMX_CK(cudaGetLastError());
+    std::vector<int> flags((size_t)ns);
+    TMX_CK(cudaMemcpyAsync(flags.data(), b->d_flags, flags.size() * sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+    TMX_CK(cudaStreamSynchronize(b->stream));
+    for (int e = 0; e < n; e++) bad[e] = flags[(size_t)slots[e]];
+    return TMX_OK;
+}
+
 int tmx_batch_fields(tmx_batch* b, int slot, int box, int field, double* host_out)
 {
     if (!b || !host_out) return fail(TMX_E_INVALID, "null argument");
@@ -848,6 +880,7 @@ void tmx_batch_destroy(tmx_batch* b)
     cudaFree(b->d_counts);
     cudaFree(b->d_slots);
     cudaFree(b->d_im);
+    cudaFree(b->d_flags);
     cudaFree(b->arena_base);
     if (b->fork) cudaEventDestroy(b->fork);
     if (b->join) cudaEventDestroy(b->join);

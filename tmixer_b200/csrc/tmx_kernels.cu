@@ -83,6 +83,22 @@ __global__ void k_outlet_im_batch(const MixerDesc* __restrict__ D, const int* __
     out[3 * e + s] = ok ? 1.0 - sqrt(var / (avg * (mx - avg))) : 0.0;
 }
 
+__global__ void k_nonfinite_batch(const MixerDesc* __restrict__ D, const int4* __restrict__ blocks,
+                                  const int* __restrict__ counts, int* __restrict__ flags)
+{
+    const int nblk = counts[0];
+    for (int b = blockIdx.x; b < nblk; b += gridDim.x) {
+        const int4 cb = blocks[b];
+        const MixerDesc& d = D[cb.x];
+        const double* mac = d.X[0].mac;
+        const long long ps = d.G.ps;
+        bool bad = false;
+        for (int t = threadIdx.x; t < cb.z; t += blockDim.x)
+            for (int f = 0; f < 7; f++) bad |= !isfinite(mac[f * ps + cb.y + t]);
+        if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(&flags[cb.x], 1);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Fixed device scratch of tmx_mixing_static (no allocation in that call).
 // Every word the call reads is written earlier in the same call, so nothing

@@ -74,6 +74,11 @@ TMX_DECLARE_BATCH_KERNELS(f16)
 // out[3e..3e+2], with the arithmetic of k_mixing_rows and its finish.
 __global__ void k_outlet_im_batch(const MixerDesc* D, const int* slots, int n, double* out);
 
+// Health of batch mixers: flags[m] |= 1 for every mixer m with a non-finite
+// macroscopic value (density, velocity or concentration) in the last fields
+// written, over the batch's cell-block list (counts[0] blocks).
+__global__ void k_nonfinite_batch(const MixerDesc* D, const int4* blocks, const int* counts, int* flags);
+
 __global__ void k_mixing_rows(const double* __restrict__ Mac, Geom G, double* __restrict__ stats);
 __global__ void k_sums(const double* __restrict__ Mac, Geom G, double* __restrict__ partial);
 // Pressure and specific power of one mixer (layout of out: tmx_kernels.cu).

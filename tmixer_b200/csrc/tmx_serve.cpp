@@ -16,6 +16,8 @@
 //     last window steps, or when it reaches max_steps; its range
 //     goes back to the engine and the next waiting request fills it before
 //     the next chunk of steps;
+//   - a mixer the engine reports as non-finite (optional health callback)
+//     is retired at once with status TMX_E_NONFINITE;
 //   - with no mixer admitted, the loop idles until the next arrival.
 #include <algorithm>
 #include <array>
@@ -137,6 +139,11 @@ int tmx_serve_with(const tmx_serve_ops* ops, const tmx_request* reqs, int n, con
         std::vector<double> im(3 * active.size());
         rc = ops->outlet_im(ops->ctx, slots.data(), (int)slots.size(), im.data());
         if (rc) return rc;
+        std::vector<int> bad(active.size(), 0);
+        if (ops->health) {
+            rc = ops->health(ops->ctx, slots.data(), (int)slots.size(), bad.data());
+            if (rc) return rc;
+        }
         checks++;
         const double now = ops->now(ops->ctx);
         area += (now - last_t) * (double)active.size();
@@ -160,9 +167,9 @@ int tmx_serve_with(const tmx_serve_ops* ops, const tmx_request* reqs, int n, con
                     if (!(a.history[h][s] != 0.0)) converged = false;
             for (int s = 0; converged && s < 3; s++)
                 if (!(std::fabs(a.history.back()[s] - a.history.front()[s]) < q.tol)) converged = false;
-            if (converged || a.steps >= q.max_steps) {
+            if (bad[i] || converged || a.steps >= q.max_steps) {
                 tmx_served& o = out[a.req];
-                o.status = converged ? 0 : 1;
+                o.status = bad[i] ? TMX_E_NONFINITE : (converged ? 0 : 1);
                 o.steps = a.steps;
                 o.finished = now;
                 for (int s = 0; s < 3; s++) o.outlet_im[s] = a.history.back()[s];
@@ -212,6 +219,7 @@ int bf_add(void* ctx, const tmx_case* c, int* slot) { return tmx_batch_add(((Bat
 int bf_remove(void* ctx, int slot) { return tmx_batch_remove(((BatchCtx*)ctx)->b, slot); }
 int bf_step(void* ctx, int nsteps) { return tmx_batch_step(((BatchCtx*)ctx)->b, nsteps, 1); }
 int bf_im(void* ctx, const int* slots, int n, double* im) { return tmx_batch_outlet_im(((BatchCtx*)ctx)->b, slots, n, im); }
+int bf_health(void* ctx, const int* slots, int n, int* bad) { return tmx_batch_health(((BatchCtx*)ctx)->b, slots, n, bad); }
 double bf_now(void* ctx)
 {
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - ((BatchCtx*)ctx)->t0).count();
@@ -229,6 +237,6 @@ extern "C" int tmx_serve(tmx_batch* b, const tmx_request* reqs, int n, const tmx
 {
     if (!b) return fail(TMX_E_INVALID, "null batch");
     BatchCtx ctx{b, std::chrono::steady_clock::now()};
-    tmx_serve_ops ops{&ctx, bf_footprint, bf_capacity, bf_add, bf_remove, bf_step, bf_im, bf_now, bf_wait};
+    tmx_serve_ops ops{&ctx, bf_footprint, bf_capacity, bf_add, bf_remove, bf_step, bf_im, bf_now, bf_wait, bf_health};
     return tmx_serve_with(&ops, reqs, n, opts, out, summary);
 }
