@@ -3,6 +3,8 @@ the plain FP64 form on the same case: velocity and concentration fields within
 a relative L2 error of 1e-3, the outlet mixing index within 1e-3, density and
 the FP64 conservation sums close, and the FP16 form's stored populations,
 decoded on the host, close to the FP64 populations."""
+import dataclasses
+
 import numpy as np
 import pytest
 
@@ -80,3 +82,18 @@ def test_init_state_exact(gpu, precision):
         for b in (0, 1):
             for fld in range(4):
                 np.testing.assert_allclose(s.populations(b, fld), r.populations(b, fld), rtol=1e-6, atol=1e-7)
+
+
+@pytest.mark.parametrize("precision", [T.TMX_FP32, T.TMX_FP16])
+def test_device_inlet_profile(gpu, precision):
+    """The reduced-precision forms compute the inlet duct series on the device
+    (odd terms, sinpi); it agrees with the FP64 form's host series (the
+    reference's libm bits) to 1e-12 of the profile's maximum.  (At the far
+    walls the host's sin(m pi (1 +- eps)) leaves about 1e-17 where sinpi gives
+    exact zeros.)"""
+    spec = T.w_layout(12, u_max=0.05, tau_f=0.6, tau_c=0.6, k=1e-3, rho=1.0)
+    with T.Solver(spec) as s64, T.Solver(dataclasses.replace(spec, precision=precision)) as slp:
+        s64.init()
+        slp.init()
+        for a, b in zip(slp.inlet_profile(), s64.inlet_profile()):
+            np.testing.assert_allclose(a, b, rtol=0, atol=1e-12 * np.abs(b).max())

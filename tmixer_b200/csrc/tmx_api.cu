@@ -270,6 +270,43 @@ void inlet_scale(const tmx_case& c, const std::vector<double>& raw, double avera
     }
 }
 
+int inlet_series_device(int iny, int nz, cudaStream_t stream, std::vector<double>& raw, double& average)
+{
+    const size_t n = (size_t)(iny + 3) * (nz + 3);
+    double* d = nullptr;
+    TMX_CK(cudaMalloc((void**)&d, n * sizeof(double)));
+    cudaError_t e = cudaMemsetAsync(d, 0, n * sizeof(double), stream);
+    if (e == cudaSuccess) {
+        tmx::k_inlet_series<<<std::max(1, std::min((iny * nz + 127) / 128, 1024)), 128, 0, stream>>>(iny, nz, d);
+        e = cudaGetLastError();
+    }
+    raw.assign(n, 0.0);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(raw.data(), d, n * sizeof(double), cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    cudaFree(d);
+    TMX_CK(e);
+    const int W = nz + 3;
+    double sum = 0;
+    for (int i = 1; i <= iny; i++)
+        for (int j = 1; j <= nz; j++) sum += raw[(size_t)i * W + j];
+    average = sum / ((iny) * (nz));
+    return TMX_OK;
+}
+
+int inlet_profile_form(const tmx_case& c, cudaStream_t stream, std::vector<double>& U1, std::vector<double>& U2)
+{
+    if (c.precision == TMX_FP64) {
+        inlet_profile(c, U1, U2);
+        return TMX_OK;
+    }
+    std::vector<double> raw;
+    double average;
+    int rc = inlet_series_device(c.iny, c.nz, stream, raw, average);
+    if (rc) return rc;
+    inlet_scale(c, raw, average, U1, U2);
+    return TMX_OK;
+}
+
 void inlet_profile(const tmx_case& c, std::vector<double>& U1, std::vector<double>& U2)
 {
     std::vector<double> raw;
@@ -641,7 +678,8 @@ int tmx_init(tmx_handle* h)
 {
     if (!h) return fail(TMX_E_INVALID, "null handle");
     TMX_CK(cudaSetDevice(h->device));
-    inlet_profile(h->c, h->uin1, h->uin2);
+    int rc = inlet_profile_form(h->c, h->stream, h->uin1, h->uin2);
+    if (rc) return rc;
     if (h->tbytes == 8) {
         const size_t nu = h->uin1.size() * sizeof(double);
         TMX_CK(cudaMemcpy(h->uin_d[0], h->uin1.data(), nu, cudaMemcpyHostToDevice));

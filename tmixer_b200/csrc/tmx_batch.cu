@@ -152,20 +152,29 @@ struct Arena {
 std::mutex g_series_mu;
 std::map<std::pair<int, int>, std::pair<std::vector<double>, double>> g_series;
 
-void cached_inlet(const tmx_case& c, std::vector<double>& U1, std::vector<double>& U2)
+// (one cache per arithmetic: the host series for FP64, the device series for
+// the reduced-precision forms)
+int cached_inlet(const tmx_case& c, cudaStream_t stream, std::vector<double>& U1, std::vector<double>& U2)
 {
+    const bool host = c.precision == TMX_FP64;
     std::pair<std::vector<double>, double> e;
     {
         std::lock_guard<std::mutex> lk(g_series_mu);
-        auto it = g_series.find({c.iny, c.nz});
+        auto it = g_series.find({host ? c.iny : -c.iny, c.nz});
         if (it != g_series.end()) e = it->second;
     }
     if (e.first.empty()) {
-        inlet_series(c.iny, c.nz, e.first, e.second);
+        if (host) {
+            inlet_series(c.iny, c.nz, e.first, e.second);
+        } else {
+            int rc = inlet_series_device(c.iny, c.nz, stream, e.first, e.second);
+            if (rc) return rc;
+        }
         std::lock_guard<std::mutex> lk(g_series_mu);
-        g_series[{c.iny, c.nz}] = e;
+        g_series[{host ? c.iny : -c.iny, c.nz}] = e;
     }
     inlet_scale(c, e.first, e.second, U1, U2);
+    return TMX_OK;
 }
 
 }  // namespace
@@ -386,7 +395,8 @@ void set_grids(tmx_batch* b)
 int init_slot(tmx_batch* b, Slot& s)
 {
     std::vector<double> u1, u2;
-    cached_inlet(s.c, u1, u2);
+    int rc = cached_inlet(s.c, b->stream, u1, u2);
+    if (rc) return rc;
     if (b->K->tbytes == 8) {
         TMX_CK(cudaMemcpyAsync(s.uin[0], u1.data(), u1.size() * 8, cudaMemcpyHostToDevice, b->stream));
         TMX_CK(cudaMemcpyAsync(s.uin[1], u2.data(), u2.size() * 8, cudaMemcpyHostToDevice, b->stream));
@@ -604,7 +614,8 @@ int tmx_batch_checkpoint(tmx_batch* b, int slot, void* buf, long long bytes)
         p += sec[k];
     }
     std::vector<double> u1, u2;
-    cached_inlet(s.c, u1, u2);
+    int rc = cached_inlet(s.c, b->stream, u1, u2);
+    if (rc) return rc;
     std::memcpy(p, u1.data(), u1.size() * 8);
     std::memcpy(p + u1.size() * 8, u2.data(), u2.size() * 8);
     return TMX_OK;

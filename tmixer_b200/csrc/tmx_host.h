@@ -61,6 +61,12 @@ int boundary_list(const Geom& G, std::vector<int>& nodes, std::vector<unsigned c
 // scaling to umean and the shifts.
 void inlet_profile(const tmx_case& c, std::vector<double>& U1, std::vector<double>& U2);
 void inlet_series(int iny, int nz, std::vector<double>& raw, double& average);
+// The same series computed on the current device (k_inlet_series) with the
+// host's summation of the mean; for the reduced-precision forms.
+int inlet_series_device(int iny, int nz, cudaStream_t stream, std::vector<double>& raw, double& average);
+// The inlet profiles of a case in its form: the host series for FP64 (the
+// reference's bits), the device series otherwise.
+int inlet_profile_form(const tmx_case& c, cudaStream_t stream, std::vector<double>& U1, std::vector<double>& U2);
 void inlet_scale(const tmx_case& c, const std::vector<double>& raw, double average, std::vector<double>& U1,
                  std::vector<double>& U2);
 

@@ -100,6 +100,37 @@ __global__ void k_nonfinite_batch(const MixerDesc* __restrict__ D, const int4* _
 }
 
 // ---------------------------------------------------------------------------
+// The rectangular-duct series of GenerateInletVelocity (Tmixer.cpp:1426-1480)
+// on the device, for the reduced-precision forms: raw[(j+1)*(nz+3) + k+1] =
+// sum over m, n = 1..100 of (1 - cos m pi)(1 - cos n pi) sin(m pi j / (2 AR d))
+// sin(n pi k / (2 d)) / (m n (m^2 + AR^2 n^2)), j < iny, k < nz.  The factors
+// (1 - cos m pi) are exactly 0 for even m and 2 for odd m, so only odd m and n
+// are summed, with sinpi for the sines.  Agrees with the host's libm series to
+// about 1e-15 relative (the FP64 form keeps the host series, bit for bit).
+// ---------------------------------------------------------------------------
+__global__ void k_inlet_series(int iny, int nz, double* __restrict__ raw)
+{
+    const double d = ((nz - 1.0) / 2.0), w = ((iny - 1.0) / 2.0);
+    const double AR = (1.0 * w / d), AR2 = AR * AR;
+    const double den_m = 2.0 * AR * d, den_n = 2.0 * d;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < iny * nz; t += gridDim.x * blockDim.x) {
+        const int j = t / nz, k = t % nz;
+        double nsum = 0.0;
+        for (int n = 1; n <= 100; n += 2) {
+            const double sn = sinpi((n * (double)k) / den_n);
+            double msum = 0.0;
+            for (int m = 1; m <= 100; m += 2) {
+                const double N = 4.0 * sinpi((m * (double)j) / den_m) * sn;
+                const double D = (double)(m * n) * ((double)(m * m) + (AR2 * n * n));
+                msum += N / D;
+            }
+            nsum += msum;
+        }
+        raw[(j + 1) * (nz + 3) + (k + 1)] = nsum;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Fixed device scratch of tmx_mixing_static (no allocation in that call).
 // Every word the call reads is written earlier in the same call, so nothing
 // in it has to start at zero.

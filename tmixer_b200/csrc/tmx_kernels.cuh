@@ -81,6 +81,8 @@ __global__ void k_nonfinite_batch(const MixerDesc* D, const int4* blocks, const 
 
 __global__ void k_mixing_rows(const double* __restrict__ Mac, Geom G, double* __restrict__ stats);
 __global__ void k_sums(const double* __restrict__ Mac, Geom G, double* __restrict__ partial);
+// The inlet duct series of the reduced-precision forms, computed on the device.
+__global__ void k_inlet_series(int iny, int nz, double* __restrict__ raw);
 // Pressure and specific power of one mixer (layout of out: tmx_kernels.cu).
 __global__ void k_pressure_power(const double* __restrict__ Mac, Geom G, double tau, double* __restrict__ out);
 
