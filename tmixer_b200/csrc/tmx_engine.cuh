@@ -2,7 +2,8 @@
 // policy PR (scalar type T of the arithmetic, storage type S of the
 // populations).  The kernels that instantiate it live in tmx_kernels.cu (FP64,
 // compiled without contraction: bit-exact with the reference) and
-// tmx_kernels_lp.cu (FP32 arithmetic, FP32 or shifted-FP16 storage).
+// tmx_kernels_lp.cu (FP32 arithmetic; FP32 storage, or FP16 storage of the
+// non-equilibrium part next to FP32 moment records).
 //
 // One step of the reference (equilibrium, collision, streaming,
 // boundary_conditions, calculate_velocity_density; Tmixer.cpp:10469-10475)
@@ -104,7 +105,6 @@ struct F64 {
     }
     __device__ static T decode(const S* p, int, int, const float4*, long long, int) { return __ldg(p); }
     __device__ static void encode(S* p, T v, T) { *p = v; }
-    __device__ static T raw(const S* p) { return __ldg(p); }
     // the equilibrium polynomial of one direction given by (ex, ey, ez), with
     // the operations of eq_poly (the weight enters through feq's division)
     __device__ static T pw_dir(int ex, int ey, int ez, T, T ux, T uy, T uz)
@@ -232,7 +232,6 @@ struct F32 {
     }
     __device__ static T decode(const S* p, int, int, const float4*, long long, int) { return __ldg(p); }
     __device__ static void encode(S* p, T v, T) { *p = v; }
-    __device__ static T raw(const S* p) { return __ldg(p); }
 };
 
 // FP32 arithmetic; populations stored in FP16 as their non-equilibrium part
@@ -351,7 +350,6 @@ struct F16 {
         return __half2float(__ldg(p)) + feq(r, src_pw(q, mf, ms), q, false);
     }
     __device__ static void encode(S* p, T v, T feq) { *p = __float2half_rn(v - feq); }
-    __device__ static T raw(const S* p) { return __half2float(__ldg(p)); }
 };
 
 
@@ -389,40 +387,6 @@ __device__ __forceinline__ void collide_store(typename PR::S* __restrict__ Pout,
         if (fld == 1 || fld == 2) v = v - T(wq(q)) * rt;
         if (fld == 3) v = v + (T(wq(q)) * rt) * T(2);
         PR::encode(Pout + PR::off(fld, q, ps, g), v, feq);
-    }
-}
-
-// The four fields of a node at once, for the interleaved layouts: the same
-// arithmetic as collide_store on each field, one vector store per direction.
-template <class PR>
-__device__ __forceinline__ void collide_store4(typename PR::S* __restrict__ Pout, long long ps, int g,
-                                               const typename PR::T (&f)[19], const typename PR::T (&a)[19],
-                                               const typename PR::T (&b)[19], const typename PR::T (&c)[19],
-                                               typename PR::T rho, typename PR::T ca, typename PR::T cb,
-                                               typename PR::T cc, const typename PR::T (&poly)[19], const Phys& P,
-                                               typename PR::T rt)
-{
-    using T = typename PR::T;
-    const T r[4] = {rho, ca, cb, cc};
-    T c1[4], c2[4];
-#pragma unroll
-    for (int m = 0; m < 4; m++) {
-        c1[m] = T(P.c1[m]);
-        c2[m] = T(P.c2[m]);
-    }
-#pragma unroll
-    for (int q = 0; q < 19; q++) {
-        const T in[4] = {f[q], a[q], b[q], c[q]};
-        T v[4], feq[4];
-#pragma unroll
-        for (int m = 0; m < 4; m++) {
-            feq[m] = PR::feq(r[m], poly[q], q, false);
-            v[m] = in[m] * c1[m] + c2[m] * feq[m];
-        }
-        v[1] = v[1] - T(wq(q)) * rt;
-        v[2] = v[2] - T(wq(q)) * rt;
-        v[3] = v[3] + (T(wq(q)) * rt) * T(2);
-        PR::encode4(Pout + PR::off(0, q, ps, g), v, feq);
     }
 }
 
