@@ -13,6 +13,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/tmx.h"
@@ -229,21 +230,30 @@ void inlet_series(int iny, int nz, std::vector<double>& U1, double& average)
     const double w = ((iny - 1.0) / 2.0);
     const double AR = (1.0 * w / d);
     const double den_m = 2.0 * AR * d, den_n = 2.0 * d, AR2 = AR * AR;
-    for (int j = 0; j < iny; j++)
-        for (int k = 0; k < nz; k++) {
-            double nsum = 0;
-            for (int n = 1; n <= 100; n++) {
-                double msum = 0;
-                for (int m = 1; m <= 100; m++) {
-                    const double N = (1.0 - std::cos(m * pi)) * (1.0 - std::cos(n * pi)) *
-                                     std::sin(((m * pi) / den_m) * (j)) * std::sin(((n * pi) / den_n) * (k));
-                    const double D = m * n * ((m * m) + (AR2 * n * n));
-                    msum += (N / D);
+    // every (j, k) is an independent sum: rows are spread over host threads,
+    // each value computed exactly as a single thread would
+    auto rows = [&](int j0, int j1) {
+        for (int j = j0; j < j1; j++)
+            for (int k = 0; k < nz; k++) {
+                double nsum = 0;
+                for (int n = 1; n <= 100; n++) {
+                    double msum = 0;
+                    for (int m = 1; m <= 100; m++) {
+                        const double N = (1.0 - std::cos(m * pi)) * (1.0 - std::cos(n * pi)) *
+                                         std::sin(((m * pi) / den_m) * (j)) * std::sin(((n * pi) / den_n) * (k));
+                        const double D = m * n * ((m * m) + (AR2 * n * n));
+                        msum += (N / D);
+                    }
+                    nsum += msum;
                 }
-                nsum += msum;
+                at(U1, j + 1, k + 1) = nsum;
             }
-            at(U1, j + 1, k + 1) = nsum;
-        }
+    };
+    const int nt = std::max(1, std::min((int)std::thread::hardware_concurrency(), iny));
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nt; t++) pool.emplace_back(rows, iny * t / nt, iny * (t + 1) / nt);
+    rows(0, iny / nt);
+    for (auto& th : pool) th.join();
     double sum = 0;
     for (int i = 1; i <= iny; i++)
         for (int j = 1; j <= nz; j++) sum += at(U1, i, j);

@@ -6,6 +6,7 @@
 //
 //   tmx_run [--case reference | --case w --W 32 --umax 0.05 --tauf 0.56 --tauc 0.6 --k 1e-3 --rho 1]
 //           [--steps N] [--every M] [--out DIR] [--files] [--domain-every D] [--device D]
+//           [--precision fp64|fp32|fp16]
 //
 // With --files (and --out) it also writes the reference's Tecplot files into
 // DIR at the reference's moments: after step itr+1 for itr % every == 0,
@@ -37,6 +38,7 @@ int main(int argc, char** argv)
     std::string kind = "reference", out;
     int W = 32, device = 0;
     bool files = false;
+    int precision = TMX_FP64;
     long long steps = -1, every = 1000, domain_every = 5000;
     double umax = 0.05, tauf = 0.56, tauc = 0.6, k = 1e-3, rho = 1.0;
     for (int a = 1; a < argc; a++) {
@@ -58,6 +60,14 @@ int main(int argc, char** argv)
         else if (!std::strcmp(argv[a], "--every")) every = std::atoll(next("--every"));
         else if (!std::strcmp(argv[a], "--out")) out = next("--out");
         else if (!std::strcmp(argv[a], "--files")) files = true;
+        else if (!std::strcmp(argv[a], "--precision")) {
+            const char* v = next("--precision");
+            precision = !std::strcmp(v, "fp32") ? TMX_FP32 : !std::strcmp(v, "fp16") ? TMX_FP16 : TMX_FP64;
+            if (std::strcmp(v, "fp64") && std::strcmp(v, "fp32") && std::strcmp(v, "fp16")) {
+                std::fprintf(stderr, "tmx_run: --precision is fp64, fp32 or fp16\n");
+                return 2;
+            }
+        }
         else if (!std::strcmp(argv[a], "--domain-every")) domain_every = std::atoll(next("--domain-every"));
         else if (!std::strcmp(argv[a], "--device")) device = std::atoi(next("--device"));
         else {
@@ -75,6 +85,7 @@ int main(int argc, char** argv)
         if (steps < 0) steps = 1000;
     }
     if (every <= 0) every = steps;
+    c.precision = precision;
     tmx_handle* h = nullptr;
     if (tmx_create(&c, device, &h)) return die("create");
     const auto t0 = std::chrono::steady_clock::now();
