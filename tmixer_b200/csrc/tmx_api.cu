@@ -82,9 +82,9 @@ struct tmx_handle {
 };
 
 const StepKernels tmx_host::kForms[3] = {
-    {tmx::k_init_f64, tmx::k_bulk_f64, tmx::k_bfaces_f64, tmx::k_bedges_f64, 8, 8, false, true},
-    {tmx::k_init_f32, tmx::k_bulk_f32, tmx::k_bfaces_f32, tmx::k_bedges_f32, 4, 4, false, false},
-    {tmx::k_init_f16, tmx::k_bulk_f16, tmx::k_bfaces_f16, tmx::k_bedges_f16, 2, 4, true, false},
+    {tmx::k_init_f64, tmx::k_bulk_f64, tmx::k_bfaces_f64, tmx::k_bedges_f64, tmx::k_bound_f64, 8, 8, false, true},
+    {tmx::k_init_f32, tmx::k_bulk_f32, tmx::k_bfaces_f32, tmx::k_bedges_f32, nullptr, 4, 4, false, false},
+    {tmx::k_init_f16, tmx::k_bulk_f16, tmx::k_bfaces_f16, tmx::k_bedges_f16, nullptr, 2, 4, true, false},
 };
 
 namespace tmx_host {
@@ -419,11 +419,20 @@ int enqueue_step(tmx_handle* h, int cur, int write_macro, cudaEvent_t* ev)
     if (ev) TMX_CK(cudaEventRecord(ev[2], h->aux));
     const int nf = h->nface, ne = h->nb - h->nface;
     const int bt = tmx::kBoundaryThreadsHost, nl = tmx::kBoundaryLanesHost;  // nl threads per node
-    if (nf > 0)
-        h->K->faces<<<(nl * nf + bt - 1) / bt, bt, 0, h->aux>>>(X, h->bnode, h->bcls, nf, G, h->P, write_macro);
-    if (ne > 0)
-        h->K->edges<<<(nl * ne + bt - 1) / bt, bt, 0, h->aux2>>>(X, h->bnode + nf, h->bcls + nf, ne, G, h->P,
-                                                                 write_macro);
+    if (h->K->serial) {
+        // one launch, the edge and corner blocks first: their long per-node
+        // chains then run beside the face blocks instead of after them
+        // (W=32 FP64 step 198.5 us against 203.4 us as two launches)
+        const int eb = (nl * ne + bt - 1) / bt, fb = (nl * nf + bt - 1) / bt;
+        if (eb + fb > 0)
+            h->K->bound<<<eb + fb, bt, 0, h->aux>>>(X, h->bnode, h->bcls, nf, ne, eb, G, h->P, write_macro);
+    } else {
+        if (nf > 0)
+            h->K->faces<<<(nl * nf + bt - 1) / bt, bt, 0, h->aux>>>(X, h->bnode, h->bcls, nf, G, h->P, write_macro);
+        if (ne > 0)
+            h->K->edges<<<(nl * ne + bt - 1) / bt, bt, 0, h->aux2>>>(X, h->bnode + nf, h->bcls + nf, ne, G, h->P,
+                                                                     write_macro);
+    }
     TMX_CK(cudaEventRecord(h->join2, h->aux2));
     if (ev) {  // the boundary time spans both boundary kernels
         TMX_CK(cudaStreamWaitEvent(h->aux, h->join2, 0));

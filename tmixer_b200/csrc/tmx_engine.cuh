@@ -1332,9 +1332,9 @@ __device__ __forceinline__ void boundary_any(const StepPtrs& X, const Geom& G, c
 template <class PR, bool FACES>
 __device__ __forceinline__ void boundary_node(const StepPtrs& X, const int* __restrict__ bnode,
                                               const unsigned char* __restrict__ bcls, int nb, const Geom& G,
-                                              const Phys& P, int write_macro, typename PR::T (*buf)[76])
+                                              const Phys& P, int write_macro, typename PR::T (*buf)[76], int blk)
 {
-    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+    const int gt = blk * blockDim.x + threadIdx.x;
     const int t = gt >> 2, fld = gt & 3;
     // the four lanes of a node share one warp; whole nodes drop out together
     const unsigned mask = __ballot_sync(0xffffffffu, t < nb);
@@ -1370,13 +1370,27 @@ __device__ __forceinline__ void bulk_any(const StepPtrs& X, const Geom& G, const
         StepPtrs X, const int* bnode, const unsigned char* bcls, int nb, Geom G, Phys P, int write_macro)       \
     {                                                                                                           \
         __shared__ PR::T buf[PR::kOnePass ? kBoundaryThreads / 4 : 1][76];                                                         \
-        boundary_node<PR, true>(X, bnode, bcls, nb, G, P, write_macro, buf);                                    \
+        boundary_node<PR, true>(X, bnode, bcls, nb, G, P, write_macro, buf, blockIdx.x);                        \
     }                                                                                                           \
     __global__ void __launch_bounds__(kBoundaryThreads) k_bedges_##NAME(                                       \
         StepPtrs X, const int* bnode, const unsigned char* bcls, int nb, Geom G, Phys P, int write_macro)       \
     {                                                                                                           \
         __shared__ PR::T buf[PR::kOnePass ? kBoundaryThreads / 4 : 1][76];                                                         \
-        boundary_node<PR, false>(X, bnode, bcls, nb, G, P, write_macro, buf);                                   \
+        boundary_node<PR, false>(X, bnode, bcls, nb, G, P, write_macro, buf, blockIdx.x);                       \
+    }
+
+// Faces and edges in one launch, the first eblocks blocks on the edge and
+// corner list (bnode + nf), the rest on the face list (the FP64 step, whose
+// bulk kernel follows the boundary).
+#define TMX_DEFINE_BOUND_KERNEL(PR, NAME)                                                                         \
+    __global__ void __launch_bounds__(kBoundaryThreads) k_bound_##NAME(StepPtrs X, const int* bnode,           \
+        const unsigned char* bcls, int nf, int ne, int eblocks, Geom G, Phys P, int write_macro)                 \
+    {                                                                                                           \
+        __shared__ PR::T buf[PR::kOnePass ? kBoundaryThreads / 4 : 1][76];                                      \
+        if ((int)blockIdx.x < eblocks)                                                                          \
+            boundary_node<PR, false>(X, bnode + nf, bcls + nf, ne, G, P, write_macro, buf, blockIdx.x);         \
+        else                                                                                                    \
+            boundary_node<PR, true>(X, bnode, bcls, nf, G, P, write_macro, buf, blockIdx.x - eblocks);          \
     }
 
 

@@ -35,6 +35,8 @@ struct StepKernels {
     void (*bulk)(tmx::StepPtrs, Geom, Phys, int);
     void (*faces)(tmx::StepPtrs, const int*, const unsigned char*, int, Geom, Phys, int);
     void (*edges)(tmx::StepPtrs, const int*, const unsigned char*, int, Geom, Phys, int);
+    // faces and edges in one launch (serial forms only)
+    void (*bound)(tmx::StepPtrs, const int*, const unsigned char*, int, int, int, Geom, Phys, int);
     int sbytes, tbytes;
     bool moments;  // the form stores per-node FP32 moments next to the populations
     bool serial;   // the bulk kernel runs after the boundary kernels, not beside them

@@ -36,6 +36,8 @@ constexpr int kBoundaryLanesHost = 4;      // threads per boundary node (one per
 TMX_DECLARE_STEP_KERNELS(f64)
 TMX_DECLARE_STEP_KERNELS(f32)
 TMX_DECLARE_STEP_KERNELS(f16)
+__global__ void k_bound_f64(StepPtrs X, const int* bnode, const unsigned char* bcls, int nf, int ne, int eblocks,
+                            Geom G, Phys P, int write_macro);
 
 // One mixer of a batch: its buffers for either parity of the batch's step
 // counter, its geometry and its physics constants (device memory, read by
