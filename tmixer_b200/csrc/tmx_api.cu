@@ -75,6 +75,7 @@ struct tmx_handle {
     cudaStream_t aux = nullptr, aux2 = nullptr;
     cudaEvent_t fork = nullptr, join = nullptr, join2 = nullptr;
     int nface = 0;  // the first nface boundary nodes are face classes
+    int nwall = 0;  // the last nwall are wall faces (StepKernels::walls)
     // one captured step per (state buffer, macroscopic output) combination
     cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
     int sbytes = 8, tbytes = 8;  // storage / arithmetic bytes per value of the form
@@ -82,9 +83,9 @@ struct tmx_handle {
 };
 
 const StepKernels tmx_host::kForms[3] = {
-    {tmx::k_init_f64, tmx::k_bulk_f64, tmx::k_bfaces_f64, tmx::k_bedges_f64, tmx::k_bound_f64, 8, 8, false, true},
-    {tmx::k_init_f32, tmx::k_bulk_f32, tmx::k_bfaces_f32, tmx::k_bedges_f32, nullptr, 4, 4, false, false},
-    {tmx::k_init_f16, tmx::k_bulk_f16, tmx::k_bfaces_f16, tmx::k_bedges_f16, nullptr, 2, 4, true, false},
+    {tmx::k_init_f64, tmx::k_bulk_f64, tmx::k_bfaces_f64, tmx::k_bedges_f64, tmx::k_bound_f64, tmx::k_walls_f64, 8, 8, false, true},
+    {tmx::k_init_f32, tmx::k_bulk_f32, tmx::k_bfaces_f32, tmx::k_bedges_f32, nullptr, nullptr, 4, 4, false, false},
+    {tmx::k_init_f16, tmx::k_bulk_f16, tmx::k_bfaces_f16, tmx::k_bedges_f16, nullptr, nullptr, 2, 4, true, false},
 };
 
 namespace tmx_host {
@@ -326,7 +327,7 @@ void inlet_profile(const tmx_case& c, std::vector<double>& U1, std::vector<doubl
 }
 
 int boundary_list(const Geom& G, std::vector<int>& nodes, std::vector<unsigned char>& cls, int& nface,
-                  std::vector<int>* class_count)
+                  std::vector<int>* class_count, int* nwall)
 {
     std::vector<std::pair<int, int>> bl;
     bl.reserve((size_t)boundary_count(G));
@@ -338,19 +339,34 @@ int boundary_list(const Geom& G, std::vector<int>& nodes, std::vector<unsigned c
                     if (!tmx::is_boundary(G, b, i, j, k)) continue;
                     const int c = classify(G, b, i, j, k);
                     if (c < 0) return fail(TMX_E_INVALID, "internal: boundary node (%d,%d,%d,%d) has no class", b, i, j, k);
-                    // faces first, then edges and corners; by class, then node
-                    bl.emplace_back((tmx::is_face_class(c) ? 0 : 256) + c, tmx::node_index(G, b, i, j, k));
+                    const int w = tmx::wall_class(G, b, i, j, k);
+                    if (w != (tmx::is_wall_class(c) ? c : -1))
+                        return fail(TMX_E_INVALID, "internal: wall class %d of node (%d,%d,%d,%d), class %d", w, b, i,
+                                    j, k, c);
                     if (class_count) (*class_count)[c]++;
+                    // faces first, then edges and corners (then, with nwall,
+                    // the wall faces); by class, then node
+                    const int key = (nwall && w >= 0) ? 512 : (tmx::is_face_class(c) ? 0 : 256) + c;
+                    bl.emplace_back(key, tmx::node_index(G, b, i, j, k));
                 }
     std::sort(bl.begin(), bl.end());
     nodes.resize(bl.size());
     cls.resize(bl.size());
     nface = 0;
+    int nw = 0;
     for (size_t t = 0; t < bl.size(); t++) {
-        cls[t] = (unsigned char)(bl[t].first & 255);
         nodes[t] = bl[t].second;
+        if (bl[t].first == 512) {  // the walls in node order
+            int b, i, j, k;
+            tmx::decode(G, nodes[t], b, i, j, k);
+            cls[t] = (unsigned char)tmx::wall_class(G, b, i, j, k);
+            nw++;
+        } else {
+            cls[t] = (unsigned char)(bl[t].first & 255);
+        }
         if (bl[t].first < 256) nface++;
     }
+    if (nwall) *nwall = nw;
     return TMX_OK;
 }
 
@@ -417,7 +433,7 @@ int enqueue_step(tmx_handle* h, int cur, int write_macro, cudaEvent_t* ev)
     TMX_CK(cudaStreamWaitEvent(h->aux, h->fork, 0));
     TMX_CK(cudaStreamWaitEvent(h->aux2, h->fork, 0));
     if (ev) TMX_CK(cudaEventRecord(ev[2], h->aux));
-    const int nf = h->nface, ne = h->nb - h->nface;
+    const int nf = h->nface, nw = h->nwall, ne = h->nb - h->nface - h->nwall;
     const int bt = tmx::kBoundaryThreadsHost, nl = tmx::kBoundaryLanesHost;  // nl threads per node
     if (h->K->serial) {
         // one launch, the edge and corner blocks first: their long per-node
@@ -426,6 +442,9 @@ int enqueue_step(tmx_handle* h, int cur, int write_macro, cudaEvent_t* ev)
         const int eb = (nl * ne + bt - 1) / bt, fb = (nl * nf + bt - 1) / bt;
         if (eb + fb > 0)
             h->K->bound<<<eb + fb, bt, 0, h->aux>>>(X, h->bnode, h->bcls, nf, ne, eb, G, h->P, write_macro);
+        if (nw > 0)
+            h->K->walls<<<(nw + bt - 1) / bt, bt, 0, h->aux2>>>(X, h->bnode + nf + ne, h->bcls + nf + ne, nw, G, h->P,
+                                                                write_macro);
     } else {
         if (nf > 0)
             h->K->faces<<<(nl * nf + bt - 1) / bt, bt, 0, h->aux>>>(X, h->bnode, h->bcls, nf, G, h->P, write_macro);
@@ -647,7 +666,7 @@ int tmx_create(const tmx_case* c, int device, tmx_handle** out)
     // boundary node list, faces first, sorted by class then node index
     std::vector<int> nodes;
     std::vector<unsigned char> cls;
-    rc = boundary_list(G, nodes, cls, h->nface, &h->class_count);
+    rc = boundary_list(G, nodes, cls, h->nface, &h->class_count, h->K->walls ? &h->nwall : nullptr);
     if (rc) {
         delete h;
         return rc;

@@ -527,7 +527,7 @@ int admit(tmx_batch* b, const tmx_case* c, const void* buf, long long size, int*
     if (off < 0)
         return fail(TMX_E_NOMEM, "batch budget: %lld bytes needed, %lld free (largest range %lld)", cv.total,
                     b->arena.free_bytes(), b->arena.largest());
-    rc = boundary_list(s.G, s.nodes, s.cls, s.nface, nullptr);
+    rc = boundary_list(s.G, s.nodes, s.cls, s.nface, nullptr, nullptr);
     if (rc) {
         b->arena.release(off, cv.total);
         return rc;

@@ -4,6 +4,8 @@
 // are identical share a class (noted per entry).
 #pragma once
 
+#include "tmx_device.cuh"
+
 namespace tmx {
 
 enum BoundaryClass : unsigned char {
@@ -48,6 +50,33 @@ __host__ __device__ constexpr bool is_face_class(int c)
 {
     return c == K_INLET1 || c == K_INLET2 || c == K_FACE_YT || c == K_FACE_Y1 || c == K_OUTLET || c == K_FACE_MX1 ||
            c == K_FACE_MXT || c == K_FACE_ZT || c == K_FACE_Z1;
+}
+
+// Wall and outlet face nodes that the FP64 bulk kernel updates itself, one
+// thread per node (the z = 1 and z = nz planes, the inlet box's y walls and
+// the outlet row; whole rows and planes, so its warps stay convergent): their
+// class, or -1.  Agrees with the host's classification for these classes; the
+// boundary list of the FP64 form leaves them out.
+__host__ __device__ inline int wall_class(const Geom& G, int b, int i, int j, int k)
+{
+    const bool zlo = k == 1, zhi = k == G.nz, zmid = !zlo && !zhi;
+    if (b == 0) {
+        if (i == 1 || i == G.inx) return -1;
+        if (j == G.iny) return zmid ? K_FACE_YT : -1;
+        if (j == 1) {
+            if (i < G.ia || i > G.ib) return zmid ? K_FACE_Y1 : -1;
+            if (i == G.ia || i == G.ib) return -1;
+        }
+        return zlo ? K_FACE_Z1 : zhi ? K_FACE_ZT : -1;
+    }
+    if (i == 1 || i == G.mnx) return -1;
+    if (j == 1) return zmid ? K_OUTLET : -1;
+    return zlo ? K_FACE_Z1 : zhi ? K_FACE_ZT : -1;
+}
+
+__host__ __device__ constexpr bool is_wall_class(int c)
+{
+    return c == K_FACE_YT || c == K_FACE_Y1 || c == K_OUTLET || c == K_FACE_ZT || c == K_FACE_Z1;
 }
 
 }  // namespace tmx

@@ -464,8 +464,7 @@ __device__ __forceinline__ void bulk_load(const typename PR::S* __restrict__ Pin
     }
 }
 
-// One interior node; returns false for a boundary node (left to the boundary
-// kernels).
+// One interior node; boundary nodes are left to the boundary kernels.
 template <class PR>
 __device__ __forceinline__ void bulk_node(const StepPtrs& X, const Geom& G, const Phys& P, int write_macro, int g)
 {
@@ -746,6 +745,62 @@ __device__ __forceinline__ void corner_closure(const BCtx<PR>& c, int fld, int n
     }
 }
 
+// Flow closures of the y and z walls, the outlet and the mixing box's x walls
+// on a node's pulled populations (the species of these faces are a copy of
+// the interior neighbour's pulls).
+template <class T>
+__device__ __forceinline__ void wall_flow_closure(int cls, T rout, T (&v)[19])
+{
+    switch (cls) {
+    case K_FACE_YT: {  // Case 10 flow (:2731-2764); species copy from y-1 (:2766-2872)
+        const T C = T(0.5) * (v[5] - v[6] + v[11] + v[12] - v[13] - v[14]);
+        v[4] = v[2]; v[16] = v[18] - C; v[17] = v[15] + C;
+        const T A = T(0.5) * (v[1] - v[3] + v[11] - v[12] - v[13] + v[14]);
+        v[9] = v[7] + A; v[10] = v[8] - A;
+    } break;
+    case K_FACE_Y1: {  // Cases 11, 12 flow (:2874-2906, :3016-3049); species copy from y+1
+        const T C = T(0.5) * (v[5] - v[6] + v[11] + v[12] - v[13] - v[14]);
+        v[2] = v[4]; v[15] = v[17] - C; v[18] = v[16] + C;
+        const T A = T(0.5) * (v[1] - v[3] + v[11] - v[12] - v[13] + v[14]);
+        v[7] = v[9] - A; v[8] = v[10] + A;
+    } break;
+    case K_OUTLET: {  // Case 13 flow (:3162-3190); species copy from y+1 (:3192-3273)
+        const T uy = T(1) - (T(1) / rout) * ((v[0] + v[1] + v[3] + v[5] + v[6] + v[11] + v[12] + v[13] + v[14]) +
+                                                T(2) * (v[4] + v[9] + v[10] + v[16] + v[17]));
+        const T A = (rout * uy) / T(6);
+        const T B = T(0.5) * ((v[3] + v[12] + v[13]) - (v[1] + v[11] + v[14]));
+        const T C = T(0.5) * ((v[6] + v[13] + v[14]) - (v[5] + v[11] + v[12]));
+        v[2] = v[4] + (rout * uy) / T(3);
+        v[7] = v[9] + (A + B); v[8] = v[10] + (A - B); v[15] = v[17] + (A + C); v[18] = v[16] + (A - C);
+    } break;
+    case K_FACE_MX1: {  // Case 14 (:3275-3404); species copy from x+1
+        const T C = T(0.5) * ((v[6] + v[17] + v[18]) - (v[5] + v[15] + v[16]));
+        v[1] = v[3]; v[11] = v[13] + (C); v[14] = v[12] - (C);
+        const T A = T(0.5) * ((v[2] + v[15] + v[18]) - (v[4] + v[16] + v[17]));
+        v[7] = v[9] - A; v[10] = v[8] + A;
+    } break;
+    case K_FACE_MXT: {  // Case 15 (:3405-3539); species copy from x-1
+        const T C = T(0.5) * ((v[6] + v[17] + v[18]) - (v[5] + v[15] + v[16]));
+        v[3] = v[1]; v[13] = v[11] - (C); v[12] = v[14] + (C);
+        const T A = T(0.5) * ((v[2] + v[15] + v[18]) - (v[4] + v[16] + v[17]));
+        v[9] = v[7] + A; v[8] = v[10] - A;
+    } break;
+    case K_FACE_ZT: {  // Cases 16, 17 and the opening nodes of 17 (:3540-3887); species copy from z-1
+        const T B = T(0.5) * (v[2] - v[4] + v[7] + v[8] - v[9] - v[10]);
+        v[6] = v[5]; v[17] = v[15] + B; v[18] = v[16] - B;
+        const T A = T(0.5) * (v[1] - v[3] + v[7] - v[8] - v[9] + v[10]);
+        v[13] = v[11] + A; v[14] = v[12] - A;
+    } break;
+    case K_FACE_Z1: {  // Cases 18, 19 and the opening nodes of 19 (:3888-4237); species copy from z+1
+        const T B = T(0.5) * (v[2] - v[4] + v[7] + v[8] - v[9] - v[10]);
+        v[5] = v[6]; v[15] = v[17] - B; v[16] = v[18] + B;
+        const T A = T(0.5) * (v[1] - v[3] + v[7] - v[8] - v[9] + v[10]);
+        v[11] = v[13] - A; v[12] = v[14] + A;
+    } break;
+    default: break;
+    }
+}
+
 // Apply the closure of class `cls` to field fld of the node in c, on v (the
 // node's pulled populations).  Closures follow the reference case by case;
 // the comments give the reference lines.  Face classes (inlets, outlet, walls)
@@ -795,66 +850,17 @@ __device__ __forceinline__ void closure_face(const BCtx<PR>& c, int cls, int fld
             v[12] = -v[14] + T(2.0 / 36.0) * cin;
         }
     } break;
-    case K_FACE_YT: {  // Case 10 flow (:2731-2764); species copy from y-1 (:2766-2872)
-        if (flow) {
-            const T C = T(0.5) * (v[5] - v[6] + v[11] + v[12] - v[13] - v[14]);
-            v[4] = v[2]; v[16] = v[18] - C; v[17] = v[15] + C;
-            const T A = T(0.5) * (v[1] - v[3] + v[11] - v[12] - v[13] + v[14]);
-            v[9] = v[7] + A; v[10] = v[8] - A;
-        } else pull_node(c, fld, c.b, c.i, c.j - 1, c.k, v);
-    } break;
-    case K_FACE_Y1: {  // Cases 11, 12 flow (:2874-2906, :3016-3049); species copy from y+1
-        if (flow) {
-            const T C = T(0.5) * (v[5] - v[6] + v[11] + v[12] - v[13] - v[14]);
-            v[2] = v[4]; v[15] = v[17] - C; v[18] = v[16] + C;
-            const T A = T(0.5) * (v[1] - v[3] + v[11] - v[12] - v[13] + v[14]);
-            v[7] = v[9] - A; v[8] = v[10] + A;
-        } else pull_node(c, fld, c.b, c.i, c.j + 1, c.k, v);
-    } break;
-    case K_OUTLET: {  // Case 13 flow (:3162-3190); species copy from y+1 (:3192-3273)
-        if (flow) {
-            const T rout = c.P->rho_out;
-            const T uy = T(1) - (T(1) / rout) * ((v[0] + v[1] + v[3] + v[5] + v[6] + v[11] + v[12] + v[13] + v[14]) +
-                                                    T(2) * (v[4] + v[9] + v[10] + v[16] + v[17]));
-            const T A = (rout * uy) / T(6);
-            const T B = T(0.5) * ((v[3] + v[12] + v[13]) - (v[1] + v[11] + v[14]));
-            const T C = T(0.5) * ((v[6] + v[13] + v[14]) - (v[5] + v[11] + v[12]));
-            v[2] = v[4] + (rout * uy) / T(3);
-            v[7] = v[9] + (A + B); v[8] = v[10] + (A - B); v[15] = v[17] + (A + C); v[18] = v[16] + (A - C);
-        } else pull_node(c, fld, c.b, c.i, c.j + 1, c.k, v);
-    } break;
-    case K_FACE_MX1: {  // Case 14 (:3275-3404)
-        if (flow) {
-            const T C = T(0.5) * ((v[6] + v[17] + v[18]) - (v[5] + v[15] + v[16]));
-            v[1] = v[3]; v[11] = v[13] + (C); v[14] = v[12] - (C);
-            const T A = T(0.5) * ((v[2] + v[15] + v[18]) - (v[4] + v[16] + v[17]));
-            v[7] = v[9] - A; v[10] = v[8] + A;
-        } else pull_node(c, fld, c.b, c.i + 1, c.j, c.k, v);
-    } break;
-    case K_FACE_MXT: {  // Case 15 (:3405-3539)
-        if (flow) {
-            const T C = T(0.5) * ((v[6] + v[17] + v[18]) - (v[5] + v[15] + v[16]));
-            v[3] = v[1]; v[13] = v[11] - (C); v[12] = v[14] + (C);
-            const T A = T(0.5) * ((v[2] + v[15] + v[18]) - (v[4] + v[16] + v[17]));
-            v[9] = v[7] + A; v[8] = v[10] - A;
-        } else pull_node(c, fld, c.b, c.i - 1, c.j, c.k, v);
-    } break;
-    case K_FACE_ZT: {  // Cases 16, 17 and the opening nodes of 17 (:3540-3887)
-        if (flow) {
-            const T B = T(0.5) * (v[2] - v[4] + v[7] + v[8] - v[9] - v[10]);
-            v[6] = v[5]; v[17] = v[15] + B; v[18] = v[16] - B;
-            const T A = T(0.5) * (v[1] - v[3] + v[7] - v[8] - v[9] + v[10]);
-            v[13] = v[11] + A; v[14] = v[12] - A;
-        } else pull_node(c, fld, c.b, c.i, c.j, c.k - 1, v);
-    } break;
-    case K_FACE_Z1: {  // Cases 18, 19 and the opening nodes of 19 (:3888-4237)
-        if (flow) {
-            const T B = T(0.5) * (v[2] - v[4] + v[7] + v[8] - v[9] - v[10]);
-            v[5] = v[6]; v[15] = v[17] - B; v[16] = v[18] + B;
-            const T A = T(0.5) * (v[1] - v[3] + v[7] - v[8] - v[9] + v[10]);
-            v[11] = v[13] - A; v[12] = v[14] + A;
-        } else pull_node(c, fld, c.b, c.i, c.j, c.k + 1, v);
-    } break;
+    case K_FACE_YT:
+    case K_FACE_Y1:
+    case K_OUTLET:
+    case K_FACE_MX1:
+    case K_FACE_MXT:
+    case K_FACE_ZT:
+    case K_FACE_Z1:
+        // the species of these faces are copied from the interior neighbour
+        // by the pull itself (face_copy_offset); only the flow is closed
+        if (flow) wall_flow_closure(cls, T(c.P->rho_out), v);
+        break;
     default: break;
     }
 }
@@ -1066,19 +1072,85 @@ __device__ __forceinline__ void face_copy_offset(int cls, int& di, int& dj, int&
 template <class PR, bool FACES>
 __device__ __forceinline__ void closed_pull(const BCtx<PR>& c, int cls, int fld, typename PR::T (&v)[19])
 {
-    if (FACES && fld > 0) {
-        int di, dj, dk;
-        face_copy_offset(cls, di, dj, dk);
-        if (di | dj | dk) {
-            pull_node(c, fld, c.b, c.i + di, c.j + dj, c.k + dk, v);
-            return;
-        }
-    }
-    pull_node(c, fld, c.b, c.i, c.j, c.k, v);
+    // one pull for the four lanes, the species lanes of a copy class from
+    // the interior neighbour: the warp runs the 19 pulls once, not once per
+    // branch
+    int di = 0, dj = 0, dk = 0;
+    if (FACES && fld > 0) face_copy_offset(cls, di, dj, dk);
+    pull_node(c, fld, c.b, c.i + di, c.j + dj, c.k + dk, v);
+    if (di | dj | dk) return;
     if (FACES)
         closure_face(c, cls, fld, v);
     else
         closure_edge(c, cls, fld, v);
+}
+
+// One wall face node (wall_class) in one thread, the four fields in the
+// order of bulk_node: the flow pulled and closed, then the species copied from
+// the interior neighbour's pulls (A and B summed first for the reaction term,
+// then pulled again to collide, then C).  The arithmetic is boundary_lane's:
+// the same sums, moments, outlet density, polynomial and collision.  One loop
+// over the six passes keeps a single copy of the pull and collision code.
+template <class PR>
+__device__ __forceinline__ void wall_node(const StepPtrs& X, const Geom& G, const Phys& P, int write_macro, int g,
+                                          int b, int i, int j, int k, int cls)
+{
+    using T = typename PR::T;
+    const typename PR::S* __restrict__ Pin = (const typename PR::S*)X.pin;
+    typename PR::S* __restrict__ Pout = (typename PR::S*)X.pout;
+    const long long ps = G.ps;
+    int di, dj, dk;
+    face_copy_offset(cls, di, dj, dk);
+    T poly[19];
+    T rho = T(0), ux = T(0), uy = T(0), uz = T(0), ca = T(0), cb = T(0), cc = T(0), rt = T(0);
+#pragma unroll 1
+    for (int s = 0; s < 6; s++) {
+        const int fld = s == 0 ? 0 : (s < 3 ? s : (s < 5 ? s - 2 : 3));  // flow, A, B, A, B, C
+        const int o = fld ? 1 : 0;
+        T v[19];
+#pragma unroll
+        for (int q = 0; q < 19; q++) {
+            const int src = pull_src(G, b, i + o * di, j + o * dj, k + o * dk, q);
+            v[q] = src >= 0 ? PR::decode(Pin + PR::off(fld, q, ps, src), fld, q, nullptr, ps, src) : T(0);
+        }
+        if (s == 0) wall_flow_closure(cls, T(P.rho_out), v);
+        T r = sum19(v);
+        if (s == 0) {
+            // the outlet row's density is pinned to rho_out (Tmixer.cpp:9575-9582)
+            if (b == 1 && j == 1) r = T(P.rho_out);
+            T sxm, sym, szm;
+            momentum(v, sxm, sym, szm);
+            ux = sxm / r;
+            uy = sym / r;
+            uz = szm / r;
+            PR::poly(ux, uy, uz, poly);
+            rho = r;
+        } else if (s == 1) {
+            ca = r;
+            continue;
+        } else if (s == 2) {
+            cb = r;
+            rt = T(P.rateconst) * ca * cb;
+            continue;
+        }
+        if (s == 5) cc = r;
+        collide_store<PR>(Pout, ps, g, fld, v, s == 3 ? ca : (s == 4 ? cb : r), poly, P, rt);
+    }
+    T* __restrict__ Rcur = (T*)X.rcur;
+    Rcur[g] = rho;
+    Rcur[ps + g] = ca;
+    Rcur[2 * ps + g] = cb;
+    Rcur[3 * ps + g] = cc;
+    if (write_macro) {
+        double* Mac = X.mac;
+        Mac[g] = rho;
+        Mac[ps + g] = ux;
+        Mac[2 * ps + g] = uy;
+        Mac[3 * ps + g] = uz;
+        Mac[4 * ps + g] = ca;
+        Mac[5 * ps + g] = cb;
+        Mac[6 * ps + g] = cc;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1391,6 +1463,19 @@ __device__ __forceinline__ void bulk_any(const StepPtrs& X, const Geom& G, const
             boundary_node<PR, false>(X, bnode + nf, bcls + nf, ne, G, P, write_macro, buf, blockIdx.x);         \
         else                                                                                                    \
             boundary_node<PR, true>(X, bnode, bcls, nf, G, P, write_macro, buf, blockIdx.x - eblocks);          \
+    }
+
+// The wall faces (wall_class), one thread per node of a node-sorted list.
+#define TMX_DEFINE_WALL_KERNEL(PR, NAME)                                                                          \
+    __global__ void __launch_bounds__(kBoundaryThreads) k_walls_##NAME(StepPtrs X, const int* wnode,           \
+        const unsigned char* wcls, int nw, Geom G, Phys P, int write_macro)                                     \
+    {                                                                                                           \
+        const int t = blockIdx.x * blockDim.x + threadIdx.x;                                                    \
+        if (t >= nw) return;                                                                                    \
+        const int g = wnode[t];                                                                                 \
+        int b, i, j, k;                                                                                         \
+        decode(G, g, b, i, j, k);                                                                               \
+        wall_node<PR>(X, G, P, write_macro, g, b, i, j, k, wcls[t]);                                            \
     }
 
 

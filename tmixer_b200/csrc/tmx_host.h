@@ -37,6 +37,8 @@ struct StepKernels {
     void (*edges)(tmx::StepPtrs, const int*, const unsigned char*, int, Geom, Phys, int);
     // faces and edges in one launch (serial forms only)
     void (*bound)(tmx::StepPtrs, const int*, const unsigned char*, int, int, int, Geom, Phys, int);
+    // the wall faces, one thread per node (null: the face kernel takes them)
+    void (*walls)(tmx::StepPtrs, const int*, const unsigned char*, int, Geom, Phys, int);
     int sbytes, tbytes;
     bool moments;  // the form stores per-node FP32 moments next to the populations
     bool serial;   // the bulk kernel runs after the boundary kernels, not beside them
@@ -55,9 +57,11 @@ long long boundary_count(const Geom& G);
 // Class of a boundary node (tmx_classes.h), -1 for a node no case covers.
 int classify(const Geom& G, int b, int i, int j, int k);
 // Boundary nodes sorted faces first, then by class, then by node index; the
-// first nface entries are face classes.  Returns TMX_OK or a failure code.
+// first nface entries are face classes.  With nwall the wall faces
+// (tmx::wall_class) come last, in node order, and *nwall counts them.
+// Returns TMX_OK or a failure code.
 int boundary_list(const Geom& G, std::vector<int>& nodes, std::vector<unsigned char>& cls, int& nface,
-                  std::vector<int>* class_count);
+                  std::vector<int>* class_count, int* nwall);
 // Inlet profiles Uin1, Uin2 ((iny+3) x (nz+3)) as the reference computes them:
 // the duct series (which depends on iny and nz only) and its mean, then the
 // scaling to umean and the shifts.

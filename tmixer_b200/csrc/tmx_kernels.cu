@@ -10,6 +10,7 @@ namespace tmx {
 
 TMX_DEFINE_STEP_KERNELS(F64, f64)
 TMX_DEFINE_BOUND_KERNEL(F64, f64)
+TMX_DEFINE_WALL_KERNEL(F64, f64)
 TMX_DEFINE_BATCH_KERNELS(F64, f64)
 
 // ---------------------------------------------------------------------------

@@ -38,6 +38,8 @@ TMX_DECLARE_STEP_KERNELS(f32)
 TMX_DECLARE_STEP_KERNELS(f16)
 __global__ void k_bound_f64(StepPtrs X, const int* bnode, const unsigned char* bcls, int nf, int ne, int eblocks,
                             Geom G, Phys P, int write_macro);
+__global__ void k_walls_f64(StepPtrs X, const int* wnode, const unsigned char* wcls, int nw, Geom G, Phys P,
+                            int write_macro);
 
 // One mixer of a batch: its buffers for either parity of the batch's step
 // counter, its geometry and its physics constants (device memory, read by
