@@ -83,7 +83,7 @@ struct tmx_handle {
 };
 
 const StepKernels tmx_host::kForms[3] = {
-    {tmx::k_init_f64, tmx::k_bulk_f64, tmx::k_bfaces_f64, tmx::k_bedges_f64, tmx::k_bound_f64, tmx::k_walls_f64, 8, 8, false, true},
+    {tmx::k_init_f64, tmx::k_bulk_f64, nullptr, nullptr, tmx::k_bound_f64, tmx::k_walls_f64, 8, 8, false, true},
     {tmx::k_init_f32, tmx::k_bulk_f32, tmx::k_bfaces_f32, tmx::k_bedges_f32, nullptr, nullptr, 4, 4, false, false},
     {tmx::k_init_f16, tmx::k_bulk_f16, tmx::k_bfaces_f16, tmx::k_bedges_f16, nullptr, nullptr, 2, 4, true, false},
 };

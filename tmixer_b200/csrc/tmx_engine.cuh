@@ -1437,17 +1437,21 @@ __device__ __forceinline__ void bulk_any(const StepPtrs& X, const Geom& G, const
     {                                                                                                           \
         for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < G.nnodes; g += gridDim.x * blockDim.x)          \
             bulk_any<PR>(X, G, P, write_macro, g);                                                              \
-    }                                                                                                           \
+    }
+
+// The face and the edge list as two launches (the FP32 and FP16-storage steps;
+// the FP64 step uses k_bound and k_walls).
+#define TMX_DEFINE_BOUNDARY_KERNELS(PR, NAME)                                                                     \
     __global__ void __launch_bounds__(kBoundaryThreads) k_bfaces_##NAME(                                       \
         StepPtrs X, const int* bnode, const unsigned char* bcls, int nb, Geom G, Phys P, int write_macro)       \
     {                                                                                                           \
-        __shared__ PR::T buf[PR::kOnePass ? kBoundaryThreads / 4 : 1][76];                                                         \
+        __shared__ PR::T buf[PR::kOnePass ? kBoundaryThreads / 4 : 1][76];                                      \
         boundary_node<PR, true>(X, bnode, bcls, nb, G, P, write_macro, buf, blockIdx.x);                        \
     }                                                                                                           \
     __global__ void __launch_bounds__(kBoundaryThreads) k_bedges_##NAME(                                       \
         StepPtrs X, const int* bnode, const unsigned char* bcls, int nb, Geom G, Phys P, int write_macro)       \
     {                                                                                                           \
-        __shared__ PR::T buf[PR::kOnePass ? kBoundaryThreads / 4 : 1][76];                                                         \
+        __shared__ PR::T buf[PR::kOnePass ? kBoundaryThreads / 4 : 1][76];                                      \
         boundary_node<PR, false>(X, bnode, bcls, nb, G, P, write_macro, buf, blockIdx.x);                       \
     }
 

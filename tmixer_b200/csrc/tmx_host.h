@@ -33,6 +33,7 @@ const char* last_error();
 struct StepKernels {
     void (*init)(tmx::StepPtrs, Geom, Phys, double);
     void (*bulk)(tmx::StepPtrs, Geom, Phys, int);
+    // the face and edge lists as two launches (forms whose bulk runs beside them)
     void (*faces)(tmx::StepPtrs, const int*, const unsigned char*, int, Geom, Phys, int);
     void (*edges)(tmx::StepPtrs, const int*, const unsigned char*, int, Geom, Phys, int);
     // faces and edges in one launch (serial forms only)

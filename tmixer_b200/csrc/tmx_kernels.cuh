@@ -27,7 +27,8 @@ constexpr int kBoundaryLanesHost = 4;      // threads per boundary node (one per
 
 #define TMX_DECLARE_STEP_KERNELS(NAME)                                                                          \
     __global__ void k_init_##NAME(StepPtrs X, Geom G, Phys P, double rho0);                                     \
-    __global__ void k_bulk_##NAME(StepPtrs X, Geom G, Phys P, int write_macro);                                 \
+    __global__ void k_bulk_##NAME(StepPtrs X, Geom G, Phys P, int write_macro);
+#define TMX_DECLARE_BOUNDARY_KERNELS(NAME)                                                                      \
     __global__ void k_bfaces_##NAME(StepPtrs X, const int* bnode, const unsigned char* bcls, int nb, Geom G,    \
                                     Phys P, int write_macro);                                                   \
     __global__ void k_bedges_##NAME(StepPtrs X, const int* bnode, const unsigned char* bcls, int nb, Geom G,    \
@@ -36,6 +37,8 @@ constexpr int kBoundaryLanesHost = 4;      // threads per boundary node (one per
 TMX_DECLARE_STEP_KERNELS(f64)
 TMX_DECLARE_STEP_KERNELS(f32)
 TMX_DECLARE_STEP_KERNELS(f16)
+TMX_DECLARE_BOUNDARY_KERNELS(f32)
+TMX_DECLARE_BOUNDARY_KERNELS(f16)
 __global__ void k_bound_f64(StepPtrs X, const int* bnode, const unsigned char* bcls, int nf, int ne, int eblocks,
                             Geom G, Phys P, int write_macro);
 __global__ void k_walls_f64(StepPtrs X, const int* wnode, const unsigned char* wcls, int nw, Geom G, Phys P,

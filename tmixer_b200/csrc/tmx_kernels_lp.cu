@@ -9,8 +9,10 @@
 namespace tmx {
 
 TMX_DEFINE_STEP_KERNELS(F32, f32)
+TMX_DEFINE_BOUNDARY_KERNELS(F32, f32)
 TMX_DEFINE_BATCH_KERNELS(F32, f32)
 TMX_DEFINE_STEP_KERNELS(F16, f16)
+TMX_DEFINE_BOUNDARY_KERNELS(F16, f16)
 TMX_DEFINE_BATCH_KERNELS(F16, f16)
 
 }  // namespace tmx
