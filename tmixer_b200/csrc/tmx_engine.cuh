@@ -69,16 +69,20 @@ __device__ __forceinline__ float poly_q_rn(int q, float ux, float uy, float uz)
 // two-wide FP32 arithmetic, on the field pairs (flow, A) and (B, C): given
 // the pulled values, the densities, w_q * poly_q (pw) and w_q * rate (wrt),
 // the equilibria f = r * pw and the post-collision values
-// o = in * c1 + c2 * f, A and B minus wrt, C plus 2 wrt.
-__device__ __forceinline__ void collide_pairs(float2 in01, float2 in23, float2 r01, float2 r23, float pw, float2 c1a,
-                                              float2 c1b, float2 c2a, float2 c2b, float wrt, float2& o01, float2& o23,
+// o = in + c2 * (f - in), A and B minus wrt, C plus 2 wrt.  (The same value
+// as in * c1 + c2 * f with c1 = 1 - c2, but rounding one small difference:
+// with c2 = 1/tau near 2, as for tau_c = 0.55, the two large terms of
+// opposite sign cost the species fields several times the FP32 rounding per
+// step.)  c1 is not used.
+__device__ __forceinline__ void collide_pairs(float2 in01, float2 in23, float2 r01, float2 r23, float pw, float2,
+                                              float2, float2 c2a, float2 c2b, float wrt, float2& o01, float2& o23,
                                               float2& f01, float2& f23)
 {
     const float2 pp = make_float2(pw, pw);
     f01 = __fmul2_rn(r01, pp);
     f23 = __fmul2_rn(r23, pp);
-    o01 = __ffma2_rn(c2a, f01, __fmul2_rn(in01, c1a));
-    o23 = __ffma2_rn(c2b, f23, __fmul2_rn(in23, c1b));
+    o01 = __ffma2_rn(c2a, __fadd2_rn(f01, make_float2(-in01.x, -in01.y)), in01);
+    o23 = __ffma2_rn(c2b, __fadd2_rn(f23, make_float2(-in23.x, -in23.y)), in23);
     o01 = __fadd2_rn(o01, make_float2(0.0f, -wrt));
     o23 = __fadd2_rn(o23, make_float2(-wrt, 2.0f * wrt));
 }
