@@ -375,7 +375,9 @@ __device__ __forceinline__ double pick_species(const double (&cin)[3][2], int fl
 // equilibrium polynomial, and store the result.  The reaction source of
 // Tmixer.cpp:9697-9761: species A and B (fld 1, 2) lose (w_q*rt)*1.0, C gains
 // (w_q*rt)*2.0 (molecular weights Ma = Mb = 1, Mp = 2, :9667).  fld may be a
-// run-time value; the arithmetic is the same either way.
+// run-time value; the arithmetic is the same either way.  The FP64 form
+// collides as the reference writes it, f*c1 + c2*feq; the FP32 and FP16-storage
+// forms as f + c2*(feq - f), the form of collide_pairs.
 template <class PR>
 __device__ __forceinline__ void collide_store(typename PR::S* __restrict__ Pout, long long ps, int g, int fld,
                                               const typename PR::T (&f)[19], typename PR::T r,
@@ -387,7 +389,7 @@ __device__ __forceinline__ void collide_store(typename PR::S* __restrict__ Pout,
 #pragma unroll
     for (int q = 0; q < 19; q++) {
         const T feq = PR::feq(r, poly[q], q, tiny);
-        T v = f[q] * c1 + c2 * feq;
+        T v = PR::kOnePass ? f[q] + c2 * (feq - f[q]) : f[q] * c1 + c2 * feq;
         if (fld == 1 || fld == 2) v = v - T(wq(q)) * rt;
         if (fld == 3) v = v + (T(wq(q)) * rt) * T(2);
         PR::encode(Pout + PR::off(fld, q, ps, g), v, feq);
