@@ -67,4 +67,7 @@ ORACLE_CASES = {
     "odd_ia": dict(ref_like(24, 6, 5, 8, 9, tau=0.65, k=2.0, rho0=1.5, rho_out=1.4, umean=0.05,
                             cin=[[0.9, 0.2], [0.1, 1.1], [0.05, 0.0]]), ia=6, taua=0.55, taub=0.62, taup=0.7),
     "min3": dict(ref_like(8, 3, 3, 3, 3, tau=0.6, k=1.0, umean=0.02), ia=3),
+    # the opening next to both inlet faces (ia = 2, ib = 6); pinned against
+    # the reference itself in test_oracle_vs_ref.py
+    "wide_opening": ref_like(7, 4, 4, 5, 5, umean=0.03),
 }

@@ -18,6 +18,9 @@ CASES = {
     "pvc_rows": (ref_like(9, 8, 3, 3, 770, umean=0.02), 6),
     "w3_pop": (w_like(3, umean=0.04, tau=0.58, tau_c=0.7, k=0.8, rho=1.2), 25),
     "species_pop": (GOLDEN_CASES["tiny_species"][0], 17),
+    # the opening (ia = 2 .. ib = 6) next to both inlet faces: the junction
+    # edges DD' and CC' share their rows with the inlet faces' neighbours
+    "wide_opening": (ref_like(7, 4, 4, 5, 5, umean=0.03), 12),
 }
 
 
