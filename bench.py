@@ -77,6 +77,71 @@ def workload_spec(form: str = "fp64"):
                       precision=T.PRECISIONS[form])
 
 
+def workload_params() -> dict:
+    """The workload's case constants without the CUDA library."""
+    w = WORKLOAD
+    return w_layout_params(w["W"], w["u_max"], w["tau_f"], w["tau_c"], w["k"], w["rho"])
+
+
+def case_nodes(p: dict) -> int:
+    return p["inx"] * p["iny"] * p["nz"] + p["mnx"] * p["mny"] * p["nz"]
+
+
+def w_layout_umean(W: int, u_max: float) -> float:
+    """The reference's Umean for a W-layout mixer whose duct profile peaks at
+    u_max, computed without the CUDA library (the reference arm must not load
+    it): the duct series of GenerateInletVelocity (Tmixer.cpp:1426-1539) for
+    iny = nz = W in its own loop order, scaled to mean 1, shifted as the
+    reference shifts it, and Umean = u_max / its maximum.  The terms with an
+    even m or n are exact zeros ((1 - cos(m*pi)) rounds to 0), so the sums
+    skip them without changing a bit; each (j, k) sum runs as a numpy vector
+    operation whose elements round exactly as the scalar loop does.  libm's
+    sin/cos (the ``math`` module) supply the same values as the host code's."""
+    import math
+
+    import numpy as np
+
+    iny = nz = int(W)
+    pi = 3.14159265358979323846
+    d = (nz - 1.0) / 2.0
+    w = (iny - 1.0) / 2.0
+    AR = 1.0 * w / d
+    den_m, den_n, AR2 = 2.0 * AR * d, 2.0 * d, AR * AR
+    odd = range(1, 101, 2)
+    one_m_cos = {m: 1.0 - math.cos(m * pi) for m in odd}
+    sj = {m: np.array([math.sin(((m * pi) / den_m) * j) for j in range(iny)]) for m in odd}
+    sk = {n: np.array([math.sin(((n * pi) / den_n) * k) for k in range(nz)]) for n in odd}
+    nsum = np.zeros((iny, nz))
+    for n in odd:
+        msum = np.zeros((iny, nz))
+        for m in odd:
+            N = ((one_m_cos[m] * one_m_cos[n]) * sj[m])[:, None] * sk[n][None, :]
+            D = float(m * n * ((m * m) + (AR2 * n * n)))
+            msum = msum + N / D
+        nsum = nsum + msum
+    # the average in the host's order: rows j, then columns k, one at a time
+    s = 0.0
+    for v in nsum.ravel():
+        s += float(v)
+    average = s / (iny * nz)
+    U1 = np.zeros((iny + 3, nz + 3))
+    U1[1:iny + 1, 1:nz + 1] = nsum * (1.0 / average)
+    U1[1:iny + 1, 0:nz] = U1[1:iny + 1, 1:nz + 1].copy()
+    U1[1:iny + 1, 1] = 0.0
+    return u_max / float(U1.max())
+
+
+def w_layout_params(W: int, u_max: float, tau_f: float, tau_c: float, k: float, rho: float) -> dict:
+    """The reference's case constants (oracle/build_ref.py's parameter names)
+    of a W-layout mixer: inlet 8W x W x W, mixing 2W x 4W x W, species A at
+    inlet 1 and B at inlet 2 with c = 1, rho0 = rho_out = rho, profile maximum
+    u_max.  The same case as the library's tmx_case_wlayout, without loading
+    the library."""
+    return dict(inx=8 * W, iny=W, nz=W, mnx=2 * W, mny=4 * W, tau=float(tau_f), tau_c=float(tau_c),
+                umean=w_layout_umean(W, u_max), rateconst=float(k), rho0=float(rho), rho_out=float(rho),
+                ca_in1=1.0, ca_in2=0.0, cb_in1=0.0, cb_in2=1.0, cp_in1=0.0, cp_in2=0.0)
+
+
 def workload_ref_params(spec) -> dict:
     return dict(inx=spec.inx, iny=spec.iny, nz=spec.nz, mnx=spec.mnx, mny=spec.mny, tau=spec.tau,
                 tau_c=spec.tau_a, umean=spec.umean, rateconst=spec.rateconst, rho0=spec.rho0,
@@ -84,16 +149,17 @@ def workload_ref_params(spec) -> dict:
                 cb_in2=spec.c_in[1][1], cp_in1=spec.c_in[2][0], cp_in2=spec.c_in[2][1])
 
 
-def config_dict(spec, form: str, n_gpus: int) -> dict:
-    return {"workload": "single T-mixer W=%d (inlet %dx%dx%d + mixing %dx%dx%d, %d fluid nodes), %s"
-                        % (WORKLOAD["W"], spec.inx, spec.iny, spec.nz, spec.mnx, spec.mny, spec.nz, spec.nodes(),
-                           form),
-            "form": form, "fluid_nodes": spec.nodes(), "bbox_nodes": spec.inx * (spec.iny + spec.mny) * spec.nz,
-            "tau_f": spec.tau, "tau_f_note": "configuration says %.2f; the reference's closures diverge there"
+def config_dict(p: dict, n_gpus: int) -> dict:
+    """The workload as both arms report it (identical dicts: the form of the
+    arithmetic is the line's "form" key, not part of the workload)."""
+    return {"workload": "single T-mixer W=%d (inlet %dx%dx%d + mixing %dx%dx%d, %d fluid nodes)"
+                        % (WORKLOAD["W"], p["inx"], p["iny"], p["nz"], p["mnx"], p["mny"], p["nz"], case_nodes(p)),
+            "fluid_nodes": case_nodes(p), "bbox_nodes": p["inx"] * (p["iny"] + p["mny"]) * p["nz"],
+            "tau_f": p["tau"], "tau_f_note": "configuration says %.2f; the reference's closures diverge there"
                                              % CONFIG_TAU_F,
-            "tau_c": spec.tau_a, "k": spec.rateconst, "u_max": WORKLOAD["u_max"],
+            "tau_c": p["tau_c"], "k": p["rateconst"], "u_max": WORKLOAD["u_max"], "rho": p["rho0"],
             "solve_steps": WORKLOAD["steps"], "parallelism": "replicas x%d" % n_gpus,
-            "l2": "state (2 x 319 MB) larger than L2, no flush"}
+            "l2": "state (2 x 319 MB FP64) larger than L2, no flush"}
 
 
 # ---------------------------------------------------------------------------
@@ -200,10 +266,19 @@ class ClockSampler:
 # reference arm.  The oracle package is test infrastructure; only this
 # baseline leg runs it.
 # ---------------------------------------------------------------------------
-def reference_cpu_run(spec, budget_s: float, max_steps: int | None = None) -> dict:
+# Timed steps of the reference's CPU build, the same count in the cpu_baseline
+# leg and in the reference arm: its cost per step grows over the first
+# hundreds of steps (the species fronts spread), so both time steps 2..257 of
+# the solve, after one warm-up step.
+REF_SAMPLE_STEPS = 256
+
+
+def reference_cpu_run(params: dict, budget_s: float, steps: int = REF_SAMPLE_STEPS) -> dict:
+    """Time ``steps`` steps (after one warm-up step) of the reference's own
+    OpenMP build for the case ``params`` on all of this host's cores; fewer if
+    a probe says they would take more than ``budget_s`` seconds."""
     from oracle import build_ref, oracle as O
 
-    params = workload_ref_params(spec)
     binary = build_ref.binary_path("bench_w%d" % WORKLOAD["W"], params)
     cores = os.cpu_count() or 1
     if not os.path.exists(binary):
@@ -214,14 +289,13 @@ def reference_cpu_run(spec, budget_s: float, max_steps: int | None = None) -> di
     # probe: 1 warm-up + 2 timed steps to size the sample
     _, _, t2 = O.run_ref(binary, 3, threads=cores, warmup=1)
     per = max(t2 / 2.0, 1e-4)
-    n = int(max(3, min(budget_s / per, 400)))
-    if max_steps is not None:
-        n = max(1, min(n, max_steps))
+    n = int(max(3, min(steps, budget_s / per)))
     _, _, secs = O.run_ref(binary, n + 1, threads=cores, warmup=1)
-    value = spec.nodes() * n / secs / 1e6
+    value = case_nodes(params) * n / secs / 1e6
     return {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
-            "sample": "%d timed steps (after 1 warm-up) of the same W=%d mixer, reference OpenMP build "
-                      "(g++ -O2 -fopenmp), OMP_NUM_THREADS=%d; %.2f s" % (n, WORKLOAD["W"], cores, secs),
+            "sample": "%d timed steps (steps 2..%d of the solve, after 1 warm-up step) of the same W=%d mixer, "
+                      "reference OpenMP build (g++ -O2 -fopenmp), OMP_NUM_THREADS=%d; %.2f s"
+                      % (n, n + 1, WORKLOAD["W"], cores, secs),
             "seconds": secs, "steps": n}
 
 
@@ -348,7 +422,7 @@ def run_ours(args, dist: Dist) -> dict | None:
 
     cpu = None
     if dist.world == 1 and dist.rank == 0 and not args.no_cpu_baseline:
-        cpu = reference_cpu_run(spec, budget_s=args.cpu_budget)
+        cpu = reference_cpu_run(workload_params(), budget_s=args.cpu_budget)
     dist.close()
     if dist.rank != 0:
         return None
@@ -358,7 +432,7 @@ def run_ours(args, dist: Dist) -> dict | None:
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": {"fp64": "f64", "fp32": "f32", "fp16": "f32/f16"}[args.form],
             "data": "synthetic",
-            "config": config_dict(spec, form_text[args.form], dist.world),
+            "form": form_text[args.form], "config": config_dict(workload_params(), dist.world),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
             "gpu_launches": 3 * args.steps, "forms": forms, "reference_case": refcase, "batched": batched,
             "served": served}
@@ -466,17 +540,20 @@ def run_served(args, dist: Dist, batched_mlups: float, shape: dict) -> dict:
 
 
 def run_reference(args, dist: Dist) -> dict | None:
+    """The reference arm: the reference's own OpenMP build (oracle/_ref,
+    compiled from its source) on this host's cores, for the same case and
+    config as our arm.  Nothing here loads the CUDA library: the case
+    constants come from w_layout_params."""
     if dist.rank != 0:
         return None
-    spec = workload_spec()
-    budget = args.cpu_budget * 2
-    r = reference_cpu_run(spec, budget_s=budget, max_steps=args.steps)
+    params = workload_params()
+    r = reference_cpu_run(params, budget_s=args.ref_budget)
     if "error" in r:
         return {"impl": "reference", "unavailable": r["error"]}
     return {"impl": "reference", "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": dist.world,
             "steps": r["steps"], "warmup": 1, "ms_per_step": r["seconds"] / r["steps"] * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": config_dict(spec, "reference OpenMP CPU build", dist.world),
+            "form": "the reference's OpenMP CPU build (FP64)", "config": config_dict(params, dist.world),
             "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": "reference",
                              "sample": r["sample"]},
             "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -489,7 +566,10 @@ def main(argv=None) -> int:
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--e2e-steps", type=int, default=WORKLOAD["steps"])
-    ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of reference CPU steps")
+    ap.add_argument("--cpu-budget", type=float, default=30.0,
+                    help="at most this many seconds of reference CPU steps in the cpu_baseline leg")
+    ap.add_argument("--ref-budget", type=float, default=60.0,
+                    help="at most this many seconds of reference CPU steps in the reference arm")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--form", choices=["fp64", "fp32", "fp16"], default="fp64",
                     help="form of the main line (fp64: the plain form, bit-exact with the reference)")

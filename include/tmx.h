@@ -165,12 +165,16 @@ int tmx_mixing(tmx_handle *h, double *rows_out, double *outlet_im);
  * rows_out.  No counterpart in the reference.  For callers that must not
  * allocate while they poll the mixing quality, such as a monitor thread
  * that may not take the heap lock or a host that accounts for every byte of
- * device memory itself.
+ * device memory itself.  The call launches on the handle's stream, so such
+ * a monitor thread still uses the handle under the one-thread-at-a-time rule
+ * above: it must take turns with the thread that steps the handle.
  *   - At most 4096 rows (mny + iny <= 4096); larger cases get TMX_E_INVALID
  *     (use tmx_mixing).
  *   - The first call on each device resolves the scratch address there
  *     (cudaGetSymbolAddress); make it before capturing any stream on that
- *     device.
+ *     device.  That lookup runs once per device and process: if it fails,
+ *     every later call on that device returns the same error until the
+ *     process exits.
  *   - The scratch is shared by every handle of the process on that device:
  *     calls that overlap in time on one device race and must be serialised
  *     by the caller. */

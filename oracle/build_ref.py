@@ -31,7 +31,9 @@ import re
 import subprocess
 import sys
 
-REF_SRC = "/root/reference/Tmixer.cpp"
+# The reference source: TMX_REF_SRC names it; the default is where the
+# reference is mounted in the build container.
+REF_SRC = os.environ.get("TMX_REF_SRC", "/root/reference/Tmixer.cpp")
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT_DIR = os.path.join(HERE, "_ref")
 HARNESS = os.path.join(HERE, "ref_harness.inc")

@@ -65,3 +65,39 @@ def test_workload_spec_geometry():
 def test_measured_peaks_present_or_fallback():
     p = bench.measured_peaks()
     assert p["hbm_gbs"] > 1000 and p["source"] in ("measured", "fallback")
+
+
+@pytest.mark.parametrize("W,u_max,tau_f,tau_c,k,rho", [(4, 0.05, 0.6, 0.6, 1e-3, 1.0), (8, 0.03, 0.7, 0.55, 5e-4, 1.0),
+                                                     (32, 0.05, 0.6, 0.6, 1e-3, 1.0), (48, 0.08, 0.6, 0.52, 1e-2, 1.0)])
+def test_w_layout_params_match_library(W, u_max, tau_f, tau_c, k, rho):
+    """The reference arm's case constants, computed without the CUDA library,
+    are bit for bit the library's tmx_case_wlayout (a host-only call)."""
+    import tmixer_b200 as T
+
+    want = bench.workload_ref_params(T.w_layout(W, u_max, tau_f, tau_c, k, rho))
+    got = bench.w_layout_params(W, u_max, tau_f, tau_c, k, rho)
+    assert got.keys() == want.keys()
+    for key in want:
+        assert float(got[key]).hex() == float(want[key]).hex(), key
+
+
+def test_reference_arm_does_not_load_the_library():
+    """The reference arm's case and config come from plain Python: building
+    them in a fresh interpreter imports no tmixer_b200 module and maps no
+    library of the package."""
+    import json
+    import subprocess
+    import sys
+
+    code = ("import sys, json, bench\n"
+            "p = bench.workload_params(); c = bench.config_dict(p, 1)\n"
+            "maps = open('/proc/self/maps').read()\n"
+            "print(json.dumps({'mods': [m for m in sys.modules if m.startswith('tmixer_b200')],"
+            " 'libtmx': 'libtmx' in maps, 'config': c}))\n")
+    root = os.path.dirname(os.path.abspath(bench.__file__))
+    out = subprocess.run([sys.executable, "-c", code], cwd=root, capture_output=True, text=True, check=True)
+    r = json.loads(out.stdout.strip().splitlines()[-1])
+    assert r["mods"] == [] and r["libtmx"] is False
+    # the same config dict as our arm's (which builds it from the same params)
+    assert r["config"] == json.loads(json.dumps(bench.config_dict(bench.workload_params(), 1)))
+    assert r["config"]["fluid_nodes"] == 524288

@@ -1,6 +1,6 @@
 """The oracle against the reference binary itself, including all 76
 post-step populations of every node, on cases the fixtures do not cover.
-Runs where the reference binaries exist (built here from /root/reference by
+Runs where the reference binaries exist (built from the reference source by
 oracle/build_ref.py; prebuilt binaries travel with the repository)."""
 import glob
 import os

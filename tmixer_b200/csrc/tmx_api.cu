@@ -543,6 +543,21 @@ int check_case(const tmx_case& cc)
     return TMX_OK;
 }
 
+// Two cases are the same solve: every field equal (the struct's padding
+// bytes are not compared, so a case filled member by member matches one
+// cleared with memset first).  Doubles compare by their bits.
+static bool same_case(const tmx_case& a, const tmx_case& b)
+{
+    auto same = [](double x, double y) { return std::memcmp(&x, &y, sizeof x) == 0; };
+    bool eq = a.inx == b.inx && a.iny == b.iny && a.nz == b.nz && a.mnx == b.mnx && a.mny == b.mny && a.ia == b.ia &&
+              a.precision == b.precision && same(a.tau, b.tau) && same(a.tau_a, b.tau_a) && same(a.tau_b, b.tau_b) &&
+              same(a.tau_c, b.tau_c) && same(a.rho0, b.rho0) && same(a.rho_out, b.rho_out) &&
+              same(a.rateconst, b.rateconst) && same(a.umean, b.umean);
+    for (int s = 0; s < 3; s++)
+        for (int n = 0; n < 2; n++) eq = eq && same(a.c_in[s][n], b.c_in[s][n]);
+    return eq;
+}
+
 int checkpoint_check(const void* buf, long long size, const tmx_case& c, const Geom& G)
 {
     if (size < (long long)sizeof(CheckpointHeader)) return fail(TMX_E_INVALID, "checkpoint too small");
@@ -552,7 +567,7 @@ int checkpoint_check(const void* buf, long long size, const tmx_case& c, const G
     if (hd.abi != TMX_ABI_VERSION) return fail(TMX_E_INVALID, "checkpoint of ABI %d, library %d", hd.abi, TMX_ABI_VERSION);
     if (hd.precision != c.precision)
         return fail(TMX_E_INVALID, "checkpoint of precision %d, target %d", hd.precision, c.precision);
-    if (std::memcmp(&hd.c, &c, sizeof c) != 0) return fail(TMX_E_INVALID, "checkpoint of a different case");
+    if (!same_case(hd.c, c)) return fail(TMX_E_INVALID, "checkpoint of a different case");
     long long b[5];
     checkpoint_sections(G, c.precision, b);
     if (hd.ps != G.ps || std::memcmp(hd.bytes, b, sizeof b) != 0 || size != checkpoint_total(b))
