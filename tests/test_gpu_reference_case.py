@@ -1,8 +1,9 @@
 """The reference's own hard-coded case at full size (inlet 401x51x51 +
-mixing 101x750x51, 4.9M nodes): after 100 steps every field of both boxes
-and the mixing rows equal the compiled reference's, bit for bit (digests in
-tests/golden/reference_case_100.json, made by tests/golden/make_golden.py
---full), and repeated runs of every form give the same bits."""
+mixing 101x750x51, 4.9M nodes): after 100 and after 1,000 steps every field
+of both boxes and the mixing rows equal the compiled reference's, bit for bit
+(digests in tests/golden/reference_case_<steps>.json, made by
+tests/golden/make_golden.py --full <steps>), and repeated runs of every form
+give the same bits."""
 import json
 import os
 
@@ -14,12 +15,14 @@ from tests.golden.make_golden import digest
 
 pytestmark = pytest.mark.gpu
 
-GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_case_100.json")
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_case_%d.json")
 
 
-def test_reference_case_bit_exact(gpu):
-    with open(GOLDEN) as fh:
+@pytest.mark.parametrize("steps", [100, 1000])
+def test_reference_case_bit_exact(gpu, steps):
+    with open(GOLDEN % steps) as fh:
         want = json.load(fh)
+    assert want["steps"] == steps
     with T.Solver(T.reference_case()) as s:
         s.init()
         s.step(want["steps"])

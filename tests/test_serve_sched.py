@@ -189,3 +189,43 @@ def test_non_finite_mixer_retired_and_backfilled():
     assert res[1]["admitted"] == res[0]["finished"]  # back-filled at once
     # a diverged solve has no time to solution
     assert summ["p99_s"] == res[1]["time_to_solution"]
+
+
+class PickyEngine(FakeEngine):
+    """A fake engine that refuses (TMX_E_INVALID) every case of width 6."""
+
+    def add(self, s):
+        if s.iny == 6:
+            return -1
+        return super().add(s)
+
+
+def test_refused_case_fails_alone():
+    """A request the engine cannot take (an invalid case, a precision other
+    than the batch's) is finished with the engine's error code; the loop goes
+    on with the others."""
+    reqs = [T.Request(spec(4, 300.0), 0.0), T.Request(spec(6, 300.0), 0.0), T.Request(spec(4, 400.0), 0.0)]
+    eng = PickyEngine(capacity=10**9)
+    res, summ = T.serve_with(eng, reqs, check_every=CHECK)
+    assert res[1]["status"] == -1 and res[1]["steps"] == 0
+    assert res[0]["status"] == "converged" and res[2]["status"] == "converged"
+    assert not eng.slots
+
+
+class FailingEngine(FakeEngine):
+    """A fake engine whose step fails once the clock passes 1e-3 s."""
+
+    def step(self, n):
+        if self.clock > 1e-3:
+            raise RuntimeError("device lost")
+        super().step(n)
+
+
+def test_engine_error_releases_active_slots():
+    """An error of the engine's step ends the loop with that error, after
+    every admitted mixer has been removed from the engine."""
+    reqs = [T.Request(spec(4, 300.0 + 10 * i), 0.0) for i in range(3)]
+    eng = FailingEngine(capacity=10**9)
+    with pytest.raises(RuntimeError, match="device lost"):
+        T.serve_with(eng, reqs, check_every=CHECK)
+    assert len(eng.admissions) == 3 and not eng.slots

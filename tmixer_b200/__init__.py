@@ -559,8 +559,9 @@ def serve(batch: "Batch", requests, check_every: int = 100, max_active: int = 0)
 
 def serve_with(engine, requests, check_every: int = 100, max_active: int = 0):
     """Run the same request loop (tmx_serve_with) over a Python engine object
-    with methods footprint(spec), capacity(), add(spec) -> slot or None when it
-    does not fit now, remove(slot), step(n), outlet_im(slots) -> (n, 3),
+    with methods footprint(spec), capacity(), add(spec) -> slot, None when it
+    does not fit now, or a negative TMX_E_* code when it cannot take the case
+    at all, remove(slot), step(n), outlet_im(slots) -> (n, 3),
     now(), wait_until(t), and optionally health(slots) -> list of 0/1 (1: the
     mixer's state is non-finite).  For tests of the scheduler without a GPU."""
     reqs = list(requests)
@@ -583,6 +584,8 @@ def serve_with(engine, requests, check_every: int = 100, max_active: int = 0):
         s = engine.add(CaseSpec.from_c(c.contents))
         if s is None:
             return -2
+        if int(s) < 0:  # the engine refuses this case (a TMX_E_* code)
+            return int(s)
         slot[0] = int(s)
         return 0
 

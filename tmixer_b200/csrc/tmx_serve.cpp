@@ -18,6 +18,12 @@
 //     the next chunk of steps;
 //   - a mixer the engine reports as non-finite (optional health callback)
 //     is retired at once with status TMX_E_NONFINITE;
+//   - a request the engine cannot take at all (its footprint or add callback
+//     fails with anything but TMX_E_NOMEM: an invalid case, a precision
+//     other than the batch's) is finished at once with that error code as
+//     its status, and the loop goes on with the others;
+//   - an error of step, outlet_im, health or remove ends the loop with that
+//     code, after every admitted mixer has been removed from the engine;
 //   - with no mixer admitted, the loop idles until the next arrival.
 #include <algorithm>
 #include <array>
@@ -83,6 +89,12 @@ int tmx_serve_with(const tmx_serve_ops* ops, const tmx_request* reqs, int n, con
     }
     const long long cap = ops->capacity(ops->ctx);
     std::vector<Active> active;
+    // a fatal engine error: give every admitted range back, then report it
+    auto abort_with = [&](int code) {
+        for (const Active& a : active) ops->remove(ops->ctx, a.slot);
+        active.clear();
+        return code;
+    };
     size_t next = 0;  // next request (in arrival order) not yet admitted
     int done = 0;
     long long lups = 0, checks = 0;
@@ -98,18 +110,19 @@ int tmx_serve_with(const tmx_serve_ops* ops, const tmx_request* reqs, int n, con
             if (opts->max_active > 0 && (int)active.size() >= opts->max_active) break;
             long long fp = 0;
             int rc = ops->footprint(ops->ctx, &q.c, &fp);
-            if (rc) return rc;
-            if (fp > cap) {  // can never fit
-                out[r].status = TMX_E_NOMEM;
+            if (rc == TMX_OK && fp > cap) rc = TMX_E_NOMEM;  // can never fit
+            int slot = -1;
+            if (rc == TMX_OK) {
+                rc = ops->add(ops->ctx, &q.c, &slot);
+                if (rc == TMX_E_NOMEM) break;  // wait for a retirement
+            }
+            if (rc) {  // this request cannot be served; the others go on
+                out[r].status = rc;
                 out[r].admitted = out[r].finished = t;
                 done++;
                 next++;
                 continue;
             }
-            int slot = -1;
-            rc = ops->add(ops->ctx, &q.c, &slot);
-            if (rc == TMX_E_NOMEM) break;  // wait for a retirement
-            if (rc) return rc;
             t = ops->now(ops->ctx);
             out[r].slot = slot;
             out[r].admitted = t;
@@ -133,16 +146,16 @@ int tmx_serve_with(const tmx_serve_ops* ops, const tmx_request* reqs, int n, con
         most = std::max(most, (int)active.size());
         // one chunk of steps for every admitted mixer
         int rc = ops->step(ops->ctx, every);
-        if (rc) return rc;
+        if (rc) return abort_with(rc);
         std::vector<int> slots(active.size());
         for (size_t i = 0; i < active.size(); i++) slots[i] = active[i].slot;
         std::vector<double> im(3 * active.size());
         rc = ops->outlet_im(ops->ctx, slots.data(), (int)slots.size(), im.data());
-        if (rc) return rc;
+        if (rc) return abort_with(rc);
         std::vector<int> bad(active.size(), 0);
         if (ops->health) {
             rc = ops->health(ops->ctx, slots.data(), (int)slots.size(), bad.data());
-            if (rc) return rc;
+            if (rc) return abort_with(rc);
         }
         checks++;
         const double now = ops->now(ops->ctx);
@@ -174,7 +187,12 @@ int tmx_serve_with(const tmx_serve_ops* ops, const tmx_request* reqs, int n, con
                 o.finished = now;
                 for (int s = 0; s < 3; s++) o.outlet_im[s] = a.history.back()[s];
                 rc = ops->remove(ops->ctx, a.slot);
-                if (rc) return rc;
+                if (rc) {
+                    // the failed slot stays the engine's; the others go back
+                    for (size_t k = i + 1; k < active.size(); k++) keep.push_back(active[k]);
+                    active.swap(keep);
+                    return abort_with(rc);
+                }
                 last_finish = std::max(last_finish, now);
                 done++;
             } else {
