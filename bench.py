@@ -481,13 +481,13 @@ def run_batched(args, dist: Dist, fp64_mlups: float, peaks: dict) -> dict:
     with T.Batch(T.TMX_FP16, budget=budget, device=dist.local_rank) as B:
         for s in specs:
             B.add(s)
-        tuned = B.tune(steps_per_trial=5)
+        tuned = B.tune(steps_per_trial=20)
         B.step(args.warmup, write_macro=False)
         B.sync()
         ms = B.time_steps(args.batched_steps)
         B.step(1, write_macro=True)
         im = B.outlet_im()
-        info = B.info()
+        B_shape = B.shape()
     mlups = nodes * args.batched_steps / (ms * 1e-3) / 1e6
     bpl = FORM_BYTES["fp16"]
     gbs = mlups * 1e6 * bpl / 1e9
@@ -496,7 +496,7 @@ def run_batched(args, dist: Dist, fp64_mlups: float, peaks: dict) -> dict:
             "roofline": {"bound": "hbm", "achieved": gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": gbs / peaks["hbm_gbs"], "algorithmic_bytes_per_lup": bpl,
                          "frac_populations_only": mlups * 1e6 * 304 / 1e9 / peaks["hbm_gbs"]},
-            "tuned": tuned, "launch_shape": {"threads": info["threads"], "cells": info["cells"]},
+            "tuned": tuned, "launch_shape": B_shape,
             "nonfinite_outlet_im": int(sum(1 for r in im for v in r if v != v)),
             "config": "%d mixers, W from %s, u_max U[0.02,0.08], tau_f U%s (configuration U%s), tau_c U[0.52,0.7], "
                       "k log-U[1e-4,1e-2], seed %d, FP16 storage / FP32 arithmetic, one launch per kernel "
@@ -525,10 +525,16 @@ def run_served(args, dist: Dist, batched_mlups: float, shape: dict) -> dict:
     free = torch.cuda.mem_get_info(dist.local_rank)[0]
     budget = int(min(SERVED_BUDGET, free - (8 << 30)))
     with T.Batch(T.TMX_FP16, budget=budget, device=dist.local_rank) as B:
-        B.set_shape(shape["threads"], shape["cells"])  # the batched form's tuned shape
+        B.set_from(shape)  # the batched form's tuned shape
         res, summ = T.serve(B, reqs, check_every=100)
     steps = [r["steps"] for r in res]
+    bpl = FORM_BYTES["fp16"]
+    gbs = summ["mlups"] * 1e6 * bpl / 1e9
+    hbm = measured_peaks()["hbm_gbs"]
     return {"requests": len(reqs), "budget_bytes": budget, "arrival_rate_per_s": lam,
+            "roofline": {"bound": "hbm", "achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm,
+                         "algorithmic_bytes_per_lup": bpl,
+                         "what": "aggregate served MLUPS x algorithmic bytes per lattice update over the makespan"},
             "p50_time_to_solution_s": summ["p50_s"], "p99_time_to_solution_s": summ["p99_s"],
             "mlups": summ["mlups"], "makespan_s": summ["makespan_s"], "max_active": summ["max_active"],
             "mean_active": summ["mean_active"], "converged": sum(r["status"] == "converged" for r in res),
@@ -578,7 +584,7 @@ def main(argv=None) -> int:
     ap.add_argument("--no-served", action="store_true", help="skip the served form")
     ap.add_argument("--batched-mixers", type=int, default=64)
     ap.add_argument("--batched-steps", type=int, default=5000)
-    ap.add_argument("--served-requests", type=int, default=8)
+    ap.add_argument("--served-requests", type=int, default=64)
     ap.add_argument("--served-max-steps", type=int, default=50000)
 
     args = ap.parse_args(argv)

@@ -124,6 +124,7 @@ def lib() -> ctypes.CDLL:
     L.tmx_inlet_profile.argtypes = [vp, vp, vp]
     L.tmx_step_timed.argtypes = [vp, ip, P(dp), P(dp), P(dp)]
     L.tmx_counts.argtypes = [vp, P(ctypes.c_longlong)]
+    L.tmx_set_shape.argtypes = [vp, ip, ip]
     L.tmx_time_steps.argtypes = [vp, ip, P(dp)]
     L.tmx_destroy.argtypes = [vp]
     L.tmx_destroy.restype = None
@@ -144,6 +145,8 @@ def lib() -> ctypes.CDLL:
     L.tmx_batch_set_shape.argtypes = [vp, ip, ip]
     L.tmx_batch_tune.argtypes = [vp, ip, P(ip), P(ip), P(dp)]
     L.tmx_batch_time_steps.argtypes = [vp, ip, P(dp)]
+    L.tmx_batch_set_sweep.argtypes = [vp, ip, ip]
+    L.tmx_batch_shape.argtypes = [vp, P(ip)]
     L.tmx_batch_checkpoint_size.argtypes = [vp, ip, P(LL)]
     L.tmx_batch_checkpoint.argtypes = [vp, ip, vp, LL]
     L.tmx_batch_restore.argtypes = [vp, P(_CCase), vp, LL, P(ip)]
@@ -385,6 +388,13 @@ class Solver:
         _check(lib().tmx_time_steps(self._h, int(n), ctypes.byref(ms)))
         return ms.value
 
+    def set_shape(self, kind: int, zchunk: int = 8) -> "Solver":
+        """Launch shape of the interior kernel (tmx_set_shape): SHAPE_FLAT, or
+        for the FP16 form SHAPE_SWEEP8 / SHAPE_SWEEP4 with zchunk planes per
+        tile.  Every shape gives the same bits."""
+        _check(lib().tmx_set_shape(self._h, int(kind), int(zchunk)))
+        return self
+
     def counts(self) -> dict:
         o = (ctypes.c_longlong * 4)()
         _check(lib().tmx_counts(self._h, o))
@@ -486,13 +496,35 @@ class Batch:
                     steps=o[6], table_bytes=o[7])
 
     def set_shape(self, threads: int, cells: int) -> None:
+        """The flat interior kernel with this block size and cell-block size."""
         _check(lib().tmx_batch_set_shape(self._b, int(threads), int(cells)))
 
-    def tune(self, steps_per_trial: int = 10) -> dict:
+    def set_sweep(self, tile_y: int, zchunk: int) -> None:
+        """The FP16 form's sweep interior kernel: tiles of 32 x tile_y nodes
+        walked through zchunk planes."""
+        _check(lib().tmx_batch_set_sweep(self._b, int(tile_y), int(zchunk)))
+
+    def shape(self) -> dict:
+        o = (ctypes.c_int * 4)()
+        _check(lib().tmx_batch_shape(self._b, o))
+        kind = {SHAPE_FLAT: "flat", SHAPE_SWEEP8: "sweep8", SHAPE_SWEEP4: "sweep4"}[o[0]]
+        return dict(kernel=kind, threads=o[1], cells=o[2], zchunk=o[3],
+                    nodes_per_thread=(o[2] // o[1]) if o[0] == SHAPE_FLAT else o[3])
+
+    def set_from(self, shape: dict) -> None:
+        """Apply a shape() dictionary (e.g. the tuned shape of another batch)."""
+        if shape["kernel"] == "flat":
+            self.set_shape(shape["threads"], shape["cells"])
+        else:
+            self.set_sweep(8 if shape["kernel"] == "sweep8" else 4, shape["zchunk"])
+
+    def tune(self, steps_per_trial: int = 20) -> dict:
+        """Autotune the interior kernel's shape (tmx_batch_tune) and return it
+        with its time per step."""
         t, c, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
         _check(lib().tmx_batch_tune(self._b, int(steps_per_trial), ctypes.byref(t), ctypes.byref(c),
                                     ctypes.byref(ms)))
-        return dict(threads=t.value, cells=c.value, ms_per_step=ms.value)
+        return dict(self.shape(), ms_per_step=ms.value, steps_per_trial=int(steps_per_trial))
 
     def time_steps(self, n: int) -> float:
         ms = ctypes.c_double()
@@ -531,6 +563,8 @@ class Request:
         return _CRequest(self.spec.to_c(), float(self.arrival), int(self.max_steps), int(self.window),
                          float(self.tol))
 
+
+SHAPE_FLAT, SHAPE_SWEEP8, SHAPE_SWEEP4 = 0, 1, 2
 
 SERVE_STATUS = {0: "converged", 1: "max_steps", -2: "too large for the budget", -5: "non-finite"}
 
@@ -626,5 +660,5 @@ def serve_with(engine, requests, check_every: int = 100, max_active: int = 0):
     return _serve_out(reqs, res[:len(reqs)], summ)
 
 
-__all__ = ["CaseSpec", "Solver", "Batch", "Request", "serve", "serve_with", "TmxError", "FIELDS", "TMX_FP64", "TMX_FP32", "TMX_FP16", "PRECISIONS",
+__all__ = ["SHAPE_FLAT", "SHAPE_SWEEP8", "SHAPE_SWEEP4", "CaseSpec", "Solver", "Batch", "Request", "serve", "serve_with", "TmxError", "FIELDS", "TMX_FP64", "TMX_FP32", "TMX_FP16", "PRECISIONS",
            "reference_case", "w_layout", "lib"]

@@ -80,6 +80,11 @@ struct tmx_handle {
     cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
     int sbytes = 8, tbytes = 8;  // storage / arithmetic bytes per value of the form
     const struct StepKernels* K = nullptr;
+    // interior kernel shape (tmx_set_shape): TMX_SHAPE_*, planes per tile,
+    // and the sweep kernels' tile list and grid
+    int shape = TMX_SHAPE_FLAT, zchunk = 8;
+    int4* tiles = nullptr;
+    int ntiles = 0, sweep_blocks = 0;
 };
 
 const StepKernels tmx_host::kForms[3] = {
@@ -402,6 +407,8 @@ void free_all(tmx_handle* h)
     cudaFree(h->bcls);
     cudaFree(h->stats);
     cudaFree(h->partial);
+    cudaFree(h->tiles);
+    h->tiles = nullptr;
     cudaFree(h->diag);
     h->diag = nullptr;
     h->mac = h->stats = h->partial = nullptr;
@@ -469,7 +476,12 @@ int enqueue_step(tmx_handle* h, int cur, int write_macro, cudaEvent_t* ev)
         TMX_CK(cudaStreamWaitEvent(h->stream, h->join2, 0));
     }
     if (ev) TMX_CK(cudaEventRecord(ev[0], h->stream));
-    h->K->bulk<<<h->bulk_blocks, 256, 0, h->stream>>>(X, G, h->P, write_macro);
+    if (h->shape == TMX_SHAPE_SWEEP8)
+        tmx::k_sweep8_f16<<<h->sweep_blocks, 256, 0, h->stream>>>(X, G, h->P, write_macro, h->tiles, h->ntiles);
+    else if (h->shape == TMX_SHAPE_SWEEP4)
+        tmx::k_sweep4_f16<<<h->sweep_blocks, 128, 0, h->stream>>>(X, G, h->P, write_macro, h->tiles, h->ntiles);
+    else
+        h->K->bulk<<<h->bulk_blocks, 256, 0, h->stream>>>(X, G, h->P, write_macro);
     if (ev) TMX_CK(cudaEventRecord(ev[1], h->stream));
     if (!h->K->serial) {
         TMX_CK(cudaStreamWaitEvent(h->stream, h->join, 0));
@@ -724,6 +736,52 @@ int tmx_create(const tmx_case* c, int device, tmx_handle** out)
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     h->bulk_blocks = std::max(1, std::min((G.nnodes + 255) / 256, sms * 8));
     *out = h;
+    return TMX_OK;
+}
+
+int tmx_set_shape(tmx_handle* h, int kind, int zchunk)
+{
+    if (!h) return fail(TMX_E_INVALID, "null handle");
+    if (kind != TMX_SHAPE_FLAT && kind != TMX_SHAPE_SWEEP8 && kind != TMX_SHAPE_SWEEP4)
+        return fail(TMX_E_INVALID, "tmx_set_shape: unknown kind %d", kind);
+    if (kind != TMX_SHAPE_FLAT && !h->K->moments)
+        return fail(TMX_E_INVALID, "tmx_set_shape: the sweep shapes are for the FP16 form only");
+    if (kind != TMX_SHAPE_FLAT && zchunk < 1) return fail(TMX_E_INVALID, "tmx_set_shape: zchunk must be >= 1");
+    TMX_CK(cudaSetDevice(h->device));
+    TMX_CK(cudaStreamSynchronize(h->stream));
+    if (kind != TMX_SHAPE_FLAT) {
+        const int ty = kind == TMX_SHAPE_SWEEP8 ? 8 : 4;
+        std::vector<int4> t;
+        sweep_tiles(h->G, 0, ty, zchunk, t);
+        int4* d = nullptr;
+        if (!t.empty()) {
+            cudaError_t e = cudaMalloc((void**)&d, t.size() * sizeof(int4));
+            if (e == cudaSuccess) e = cudaMemcpy(d, t.data(), t.size() * sizeof(int4), cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) {
+                cudaFree(d);
+                cudaGetLastError();
+                return fail(e == cudaErrorMemoryAllocation ? TMX_E_NOMEM : TMX_E_CUDA, "tmx_set_shape: %s",
+                            cudaGetErrorString(e));
+            }
+        }
+        int per = 1, sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &per, ty == 8 ? (const void*)tmx::k_sweep8_f16 : (const void*)tmx::k_sweep4_f16, 32 * ty, 0);
+        cudaGetLastError();
+        cudaFree(h->tiles);
+        h->tiles = d;
+        h->ntiles = (int)t.size();
+        h->sweep_blocks = std::max(1, std::min(h->ntiles, sms * std::max(1, per)));
+    }
+    h->shape = kind;
+    h->zchunk = zchunk;
+    for (auto& row : h->graph)
+        for (auto& g : row)
+            if (g) {
+                cudaGraphExecDestroy(g);
+                g = nullptr;
+            }
     return TMX_OK;
 }
 

@@ -17,8 +17,10 @@
 //     addresses, so the captured step graphs stay valid while mixers come and
 //     go; they are recaptured only when a list outgrows its capacity or the
 //     tuned launch shape changes.
-//   - tmx_batch_tune times each bulk block size and cell-block size on the
-//     batch's own mixers and keeps the fastest.
+//   - tmx_batch_tune times each interior-kernel shape on the batch's own
+//     mixers and keeps the fastest: the flat kernel's block size and
+//     cell-block size, and (FP16 form) the sweep kernels' tile height and
+//     planes per tile, i.e. nodes per thread.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -194,6 +196,8 @@ struct tmx_batch {
     int cap_desc = 0;
     int4* d_blocks = nullptr;
     int cap_blocks = 0;
+    int4* d_tiles = nullptr;  // sweep kernel tiles (FP16 form)
+    int cap_tiles = 0;
     int2* d_faces = nullptr;
     int cap_faces = 0;
     int2* d_edges = nullptr;
@@ -211,10 +215,13 @@ struct tmx_batch {
     // launch shape
     int variant = 1;     // index into kBulkThreads
     int cells = 4096;    // nodes per cell block
+    int sweep = 0;       // 0: the flat kernel; 8 or 4: the sweep kernel of that tile height
+    int zchunk = 8;      // planes per sweep tile
     int sms = 148;
     int grid_bulk[3] = {0, 0, 0};
+    int grid_sweep[2] = {0, 0};  // tile height 8, 4
     int grid_faces = 0, grid_edges = 0;
-    int nblocks = 0, nfaces = 0, nedges = 0, nactive = 0;
+    int nblocks = 0, nfaces = 0, nedges = 0, ntiles = 0, nactive = 0;
     cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
 };
 
@@ -279,7 +286,7 @@ MixerDesc desc_of(const tmx_batch* b, const Slot& s)
 int rebuild(tmx_batch* b)
 {
     std::vector<MixerDesc> desc(b->slots.size());
-    std::vector<int4> blocks;
+    std::vector<int4> blocks, tiles;
     std::vector<int2> faces, edges;
     int nactive = 0;
     for (size_t m = 0; m < b->slots.size(); m++) {
@@ -289,6 +296,7 @@ int rebuild(tmx_batch* b)
         desc[m] = desc_of(b, s);
         for (int g0 = 0; g0 < s.G.nnodes; g0 += b->cells)
             blocks.push_back(make_int4((int)m, g0, std::min(b->cells, s.G.nnodes - g0), 0));
+        if (b->sweep) sweep_tiles(s.G, (int)m, b->sweep, b->zchunk, tiles);
         for (size_t t = 0; t < s.nodes.size(); t++) {
             const int2 e = make_int2(s.nodes[t], (int)m * 256 + s.cls[t]);
             if ((int)t < s.nface)
@@ -301,6 +309,7 @@ int rebuild(tmx_batch* b)
     if (e == cudaSuccess) e = grow(b, b->d_blocks, b->cap_blocks, (int)std::max<size_t>(1, blocks.size()));
     if (e == cudaSuccess) e = grow(b, b->d_faces, b->cap_faces, (int)std::max<size_t>(1, faces.size()));
     if (e == cudaSuccess) e = grow(b, b->d_edges, b->cap_edges, (int)std::max<size_t>(1, edges.size()));
+    if (e == cudaSuccess) e = grow(b, b->d_tiles, b->cap_tiles, (int)std::max<size_t>(1, tiles.size()));
     if (e != cudaSuccess) {
         cudaGetLastError();
         return fail(e == cudaErrorMemoryAllocation ? TMX_E_NOMEM : TMX_E_CUDA, "batch tables: %s",
@@ -315,12 +324,14 @@ int rebuild(tmx_batch* b)
         TMX_CK(cudaMemcpyAsync(b->d_blocks, blocks.data(), blocks.size() * sizeof(int4), h2d, b->stream));
     if (!faces.empty()) TMX_CK(cudaMemcpyAsync(b->d_faces, faces.data(), faces.size() * sizeof(int2), h2d, b->stream));
     if (!edges.empty()) TMX_CK(cudaMemcpyAsync(b->d_edges, edges.data(), edges.size() * sizeof(int2), h2d, b->stream));
-    const int counts[3] = {(int)blocks.size(), (int)faces.size(), (int)edges.size()};
+    if (!tiles.empty()) TMX_CK(cudaMemcpyAsync(b->d_tiles, tiles.data(), tiles.size() * sizeof(int4), h2d, b->stream));
+    const int counts[4] = {(int)blocks.size(), (int)faces.size(), (int)edges.size(), (int)tiles.size()};
     TMX_CK(cudaMemcpyAsync(b->d_counts, counts, sizeof counts, h2d, b->stream));
     TMX_CK(cudaStreamSynchronize(b->stream));
     b->nblocks = counts[0];
     b->nfaces = counts[1];
     b->nedges = counts[2];
+    b->ntiles = counts[3];
     b->nactive = nactive;
     b->dirty = false;
     return TMX_OK;
@@ -342,8 +353,15 @@ int enqueue(tmx_batch* b, int parity, int write_macro)
         TMX_CK(cudaStreamWaitEvent(b->stream, b->join, 0));
         TMX_CK(cudaStreamWaitEvent(b->stream, b->join2, 0));
     }
-    b->B->bulk[b->variant]<<<b->grid_bulk[b->variant], kBulkThreads[b->variant], 0, b->stream>>>(
-        b->d_desc, b->d_blocks, b->d_counts, parity, write_macro);
+    if (b->sweep == 8)
+        tmx::k_sweep_batch8_f16<<<b->grid_sweep[0], 256, 0, b->stream>>>(b->d_desc, b->d_tiles, b->d_counts, parity,
+                                                                         write_macro);
+    else if (b->sweep == 4)
+        tmx::k_sweep_batch4_f16<<<b->grid_sweep[1], 128, 0, b->stream>>>(b->d_desc, b->d_tiles, b->d_counts, parity,
+                                                                         write_macro);
+    else
+        b->B->bulk[b->variant]<<<b->grid_bulk[b->variant], kBulkThreads[b->variant], 0, b->stream>>>(
+            b->d_desc, b->d_blocks, b->d_counts, parity, write_macro);
     TMX_CK(cudaGetLastError());
     if (!b->K->serial) {
         TMX_CK(cudaStreamWaitEvent(b->stream, b->join, 0));
@@ -383,6 +401,13 @@ void set_grids(tmx_batch* b)
         int per = 1;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void*)b->B->bulk[v], kBulkThreads[v], 0);
         b->grid_bulk[v] = b->sms * std::max(1, per);
+    }
+    if (b->K->moments) {
+        int p8 = 1, p4 = 1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p8, (const void*)tmx::k_sweep_batch8_f16, 256, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p4, (const void*)tmx::k_sweep_batch4_f16, 128, 0);
+        b->grid_sweep[0] = b->sms * std::max(1, p8);
+        b->grid_sweep[1] = b->sms * std::max(1, p4);
     }
     int pf = 1, pe = 1;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pf, (const void*)b->B->faces, tmx::kBoundaryThreadsHost, 0);
@@ -459,8 +484,8 @@ int tmx_batch_create(int precision, long long budget_bytes, int device, tmx_batc
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->join2, cudaEventDisableTiming);
-    if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_counts, 3 * sizeof(int));
-    if (e == cudaSuccess) e = cudaMemset(b->d_counts, 0, 3 * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_counts, 4 * sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(b->d_counts, 0, 4 * sizeof(int));
     if (e != cudaSuccess) {
         cudaGetLastError();
         tmx_batch_destroy(b);
@@ -797,12 +822,41 @@ int tmx_batch_set_shape(tmx_batch* b, int threads, int cells)
     if (cells < threads || cells % threads) return fail(TMX_E_INVALID, "cells per block must be a multiple of %d", threads);
     TMX_CK(cudaSetDevice(b->device));
     TMX_CK(cudaStreamSynchronize(b->stream));
-    if (v != b->variant) drop_graphs(b);
+    if (v != b->variant || b->sweep) drop_graphs(b);
     b->variant = v;
-    if (cells != b->cells) b->dirty = true;
+    if (cells != b->cells || b->sweep) b->dirty = true;
     b->cells = cells;
+    b->sweep = 0;
     return TMX_OK;
 }
+
+int tmx_batch_set_sweep(tmx_batch* b, int tile_y, int zchunk)
+{
+    if (!b) return fail(TMX_E_INVALID, "null batch");
+    if (tile_y != 8 && tile_y != 4) return fail(TMX_E_INVALID, "sweep tile height must be 8 or 4 (got %d)", tile_y);
+    if (!b->K->moments) return fail(TMX_E_INVALID, "the sweep kernels are for the FP16 form only");
+    if (zchunk < 1) return fail(TMX_E_INVALID, "planes per tile must be >= 1");
+    TMX_CK(cudaSetDevice(b->device));
+    TMX_CK(cudaStreamSynchronize(b->stream));
+    if (tile_y != b->sweep) drop_graphs(b);
+    if (tile_y != b->sweep || zchunk != b->zchunk) b->dirty = true;
+    b->sweep = tile_y;
+    b->zchunk = zchunk;
+    return TMX_OK;
+}
+
+int tmx_batch_shape(const tmx_batch* b, int out[4])
+{
+    if (!b || !out) return fail(TMX_E_INVALID, "null argument");
+    out[0] = b->sweep == 8 ? TMX_SHAPE_SWEEP8 : (b->sweep == 4 ? TMX_SHAPE_SWEEP4 : TMX_SHAPE_FLAT);
+    out[1] = b->sweep ? 32 * b->sweep : kBulkThreads[b->variant];
+    out[2] = b->cells;
+    out[3] = b->zchunk;
+    return TMX_OK;
+}
+
+// the sweep kernels' planes per tile tried by tmx_batch_tune
+constexpr int kZChunkChoices[4] = {4, 8, 16, 32};
 
 int tmx_batch_tune(tmx_batch* b, int steps_per_trial, int* threads_out, int* cells_out, double* ms_out)
 {
@@ -813,31 +867,54 @@ int tmx_batch_tune(tmx_batch* b, int steps_per_trial, int* threads_out, int* cel
     TMX_CK(cudaEventCreate(&t0));
     TMX_CK(cudaEventCreate(&t1));
     double best = 1e300;
-    int bv = b->variant, bc = b->cells;
+    int bv = b->variant, bc = b->cells, bs = b->sweep, bz = b->zchunk;
     int rc = TMX_OK;
+    // time steps_per_trial steps of the shape just set (after two steps that
+    // capture its graphs and warm up)
+    auto trial = [&](double& ms_step) {
+        rc = tmx_batch_step(b, 2, 0);
+        if (rc) return;
+        cudaEventRecord(t0, b->stream);
+        rc = tmx_batch_step(b, steps_per_trial, 0);
+        cudaEventRecord(t1, b->stream);
+        if (cudaEventSynchronize(t1) != cudaSuccess) rc = fail(TMX_E_CUDA, "tune: event wait failed");
+        float ms = 0;
+        cudaEventElapsedTime(&ms, t0, t1);
+        ms_step = ms / steps_per_trial;
+    };
     for (int v = 0; v < 3 && rc == TMX_OK; v++)
         for (int ci = 0; ci < 4 && rc == TMX_OK; ci++) {
             const int cells = kCellChoices[ci];
             if (cells < kBulkThreads[v]) continue;
             rc = tmx_batch_set_shape(b, kBulkThreads[v], cells);
-            if (rc == TMX_OK) rc = tmx_batch_step(b, 2, 0);  // capture and warm up
             if (rc) break;
-            cudaEventRecord(t0, b->stream);
-            rc = tmx_batch_step(b, steps_per_trial, 0);
-            cudaEventRecord(t1, b->stream);
-            if (cudaEventSynchronize(t1) != cudaSuccess) rc = fail(TMX_E_CUDA, "tune: event wait failed");
-            float ms = 0;
-            cudaEventElapsedTime(&ms, t0, t1);
-            if (rc == TMX_OK && ms / steps_per_trial < best) {
-                best = ms / steps_per_trial;
+            double ms = 0;
+            trial(ms);
+            if (rc == TMX_OK && ms < best) {
+                best = ms;
                 bv = v;
                 bc = cells;
+                bs = 0;
             }
         }
+    if (b->K->moments)
+        for (int ty : {8, 4})
+            for (int zi = 0; zi < 4 && rc == TMX_OK; zi++) {
+                rc = tmx_batch_set_sweep(b, ty, kZChunkChoices[zi]);
+                if (rc) break;
+                double ms = 0;
+                trial(ms);
+                if (rc == TMX_OK && ms < best) {
+                    best = ms;
+                    bs = ty;
+                    bz = kZChunkChoices[zi];
+                }
+            }
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
     if (rc) return rc;
     rc = tmx_batch_set_shape(b, kBulkThreads[bv], bc);
+    if (rc == TMX_OK && bs) rc = tmx_batch_set_sweep(b, bs, bz);
     if (rc) return rc;
     // the trials advanced the mixers: start every one of them again
     TMX_CK(cudaStreamSynchronize(b->stream));
@@ -848,8 +925,8 @@ int tmx_batch_tune(tmx_batch* b, int steps_per_trial, int* threads_out, int* cel
         }
     b->dirty = true;
     TMX_CK(cudaStreamSynchronize(b->stream));
-    if (threads_out) *threads_out = kBulkThreads[bv];
-    if (cells_out) *cells_out = bc;
+    if (threads_out) *threads_out = bs ? 32 * bs : kBulkThreads[bv];
+    if (cells_out) *cells_out = bs ? 32 * bs * bz : bc;
     if (ms_out) *ms_out = best;
     return TMX_OK;
 }
@@ -888,6 +965,7 @@ void tmx_batch_destroy(tmx_batch* b)
     cudaFree(b->d_blocks);
     cudaFree(b->d_faces);
     cudaFree(b->d_edges);
+    cudaFree(b->d_tiles);
     cudaFree(b->d_counts);
     cudaFree(b->d_slots);
     cudaFree(b->d_im);

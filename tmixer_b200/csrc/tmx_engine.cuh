@@ -205,6 +205,13 @@ struct F32 {
         v01 = make_float2(x.x, x.y);
         v23 = make_float2(x.z, x.w);
     }
+    __device__ static void decode_pairs_rec(const S* __restrict__ Pin, long long ps, int q, int, int, int, T, int s,
+                                            const float4&, const float4&, float2& v01, float2& v23)
+    {
+        const float4 x = __ldg((const float4*)(Pin + off(0, q, ps, s)));
+        v01 = make_float2(x.x, x.y);
+        v23 = make_float2(x.z, x.w);
+    }
     __device__ static void decode4(const S* __restrict__ Pin, const float4* __restrict__, long long ps, int q, int,
                                    int, int, T, int s, T (&v)[4])
     {
@@ -300,9 +307,15 @@ struct F16 {
     __device__ static void decode_pairs(const S* __restrict__ Pin, const float4* __restrict__ M, long long ps, int q,
                                         int ex, int ey, int ez, T w, int s, float2& v01, float2& v23)
     {
+        const float4 mf = __ldg(M + 2 * (long long)s), ms = __ldg(M + 2 * (long long)s + 1);
+        decode_pairs_rec(Pin, ps, q, ex, ey, ez, w, s, mf, ms, v01, v23);
+    }
+    // the same with the writer's record {mf, ms} given
+    __device__ static void decode_pairs_rec(const S* __restrict__ Pin, long long ps, int q, int ex, int ey, int ez,
+                                            T w, int s, const float4& mf, const float4& ms, float2& v01, float2& v23)
+    {
         const uint2 x = __ldg((const uint2*)(Pin + off(0, q, ps, s)));
         const float2 raw01 = __half22float2(*(const __half2*)&x.x), raw23 = __half22float2(*(const __half2*)&x.y);
-        const float4 mf = __ldg(M + 2 * (long long)s), ms = __ldg(M + 2 * (long long)s + 1);
         const float pw = __fmul_rn(poly_e_rn_t(ex, ey, ez, mf.y, mf.z, mf.w, ms.w), w);
         const float2 pp = make_float2(pw, pw);
         v01 = __fadd2_rn(raw01, __fmul2_rn(make_float2(mf.x, ms.x), pp));
@@ -549,21 +562,45 @@ __device__ __forceinline__ void bulk_node(const StepPtrs& X, const Geom& G, cons
     }
 }
 
-// One interior node for the reduced-precision forms (FP32 arithmetic): every
-// source index and (FP16 form) every writer's moments are fetched once per
-// direction and all 76 populations decoded in one pass, which the FP32
-// register budget affords (the FP64 form above loads field by field).
-template <class PR>
-__device__ __forceinline__ void bulk_node_lp(const StepPtrs& X, const Geom& G, const Phys& P, int write_macro, int g)
+// Writer records of the FP16 form for lp_interior: read from global memory at
+// the source node (the flat bulk kernel) ...
+struct RecGlobal {
+    const float4* __restrict__ M;
+    __device__ __forceinline__ void operator()(int, int s, float4& mf, float4& ms) const
+    {
+        mf = __ldg(M + 2 * (long long)s);
+        ms = __ldg(M + 2 * (long long)s + 1);
+    }
+};
+// ... or from the shared-memory planes of a sweep tile (sweep_tile): plane
+// slot (k - ez) & 3, row ty + 1 - ey, column tx + 1 - ex of (TY + 2) x 34
+// records, the two halves of each record in separate arrays.
+template <int TY>
+struct RecShared {
+    const float4* A;
+    const float4* B;
+    int tx, ty, k;
+    __device__ __forceinline__ void operator()(int q, int, float4& mf, float4& ms) const
+    {
+        const int e = (((k - EZ(q)) & 3) * (TY + 2) + ty + 1 - EY(q)) * 34 + tx + 1 - EX(q);
+        mf = A[e];
+        ms = B[e];
+    }
+};
+
+// One interior node (b, i, j, k) = g for the reduced-precision forms (FP32
+// arithmetic): every source index and (FP16 form) every writer's record
+// (from rec) is fetched once per direction and all 76 populations decoded in
+// one pass, which the FP32 register budget affords (the FP64 form loads field
+// by field).  The arithmetic does not depend on where the records come from.
+template <class PR, class Rec>
+__device__ __forceinline__ void lp_interior(const StepPtrs& X, const Geom& G, const Phys& P, int write_macro, int g,
+                                            int b, int i, int j, int k, const Rec& rec)
 {
     using T = typename PR::T;
     const typename PR::S* __restrict__ Pin = (const typename PR::S*)X.pin;
     typename PR::S* __restrict__ Pout = (typename PR::S*)X.pout;
-    const float4* __restrict__ M = X.mprev;
     const long long ps = G.ps;
-    int b, i, j, k;
-    decode(G, g, b, i, j, k);
-    if (is_boundary(G, b, i, j, k)) return;
     const int sy = box_nx(G, b), sz = box_nx(G, b) * box_ny(G, b);
     const int iface = (b == 0 && j == 1) ? 1 : ((b == 1 && j == G.mny) ? 2 : 0);
 
@@ -572,7 +609,9 @@ __device__ __forceinline__ void bulk_node_lp(const StepPtrs& X, const Geom& G, c
 #pragma unroll
     for (int q = 0; q < 19; q++) {
         const int s = bulk_src(G, g, i, k, sy, sz, iface, q);
-        PR::decode_pairs(Pin, M, ps, q, EX(q), EY(q), EZ(q), (float)wq(q), s, p01[q], p23[q]);
+        float4 mf = make_float4(0.f, 0.f, 0.f, 0.f), ms = mf;
+        if constexpr (PR::kMoments) rec(q, s, mf, ms);
+        PR::decode_pairs_rec(Pin, ps, q, EX(q), EY(q), EZ(q), (float)wq(q), s, mf, ms, p01[q], p23[q]);
     }
     // sums in index order, two fields at a time
     float2 s01 = p01[0], s23 = p23[0];
@@ -621,6 +660,103 @@ __device__ __forceinline__ void bulk_node_lp(const StepPtrs& X, const Geom& G, c
         Mac[4 * ps + g] = ca;
         Mac[5 * ps + g] = cb;
         Mac[6 * ps + g] = cc;
+    }
+}
+
+
+template <class PR>
+__device__ __forceinline__ void bulk_node_lp(const StepPtrs& X, const Geom& G, const Phys& P, int write_macro, int g)
+{
+    int b, i, j, k;
+    decode(G, g, b, i, j, k);
+    if (is_boundary(G, b, i, j, k)) return;
+    lp_interior<PR>(X, G, P, write_macro, g, b, i, j, k, RecGlobal{X.mprev});
+}
+
+// ---------------------------------------------------------------------------
+// FP16 form, interior nodes by tiles (the sweep kernels).  A block of 32 x TY
+// threads owns a tile of 32 x TY nodes of one box (x0.., y0..) and walks it
+// through the planes z0 .. z1-1, one node per thread per plane.  The writer
+// records its nodes read (the 9 source rows of each node, 19 reads per node in
+// the flat kernel) are staged once per plane in shared memory: a ring of four
+// planes of (TY + 2) x 34 records (the tile and a one-node halo), the next
+// plane but one copied asynchronously (cp.async) while the current plane is
+// computed.  The populations stream straight from global memory.  Each node's
+// arithmetic is lp_interior's, so the results are the flat kernel's bit for
+// bit.
+// ---------------------------------------------------------------------------
+constexpr int kSweepX = 32;
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
+{
+    const unsigned a = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(a), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// The node whose record a tile of box b stages at 0-based (x, y) of plane kk:
+// the node itself inside the box; on the inlet box's row y = -1 over the
+// opening the mixing box's row mny, and on the mixing box's row y = mny the
+// inlet box's row 1 (the sources of the two interface rules, as bulk_src);
+// -1 where there is no node.
+__device__ __forceinline__ int tile_rec_node(const Geom& G, int b, int x, int y, int kk)
+{
+    if (kk < 1 || kk > G.nz) return -1;
+    const int nx = box_nx(G, b), ny = box_ny(G, b);
+    if (x >= 0 && x < nx && y >= 0 && y < ny) return box_base(G, b) + ((kk - 1) * ny + y) * nx + x;
+    if (b == 0 && y == -1) {
+        const int xm = x - (G.ia - 1);
+        if (xm >= 0 && xm < G.mnx) return G.base[1] + ((kk - 1) * G.mny + (G.mny - 1)) * G.mnx + xm;
+    } else if (b == 1 && y == G.mny) {
+        const int xi = x + G.ia - 1;
+        if (xi >= 0 && xi < G.inx) return ((kk - 1) * G.iny) * G.inx + xi;
+    }
+    return -1;
+}
+
+// One tile {mixer * 2 + box, x0 | y0 << 16, z0 | z1 << 16} (0-based x0, y0;
+// interior planes z0 .. z1-1, 2 <= z0 < z1 <= nz).  A and B hold the two
+// halves of 4 * (TY + 2) * 34 records.  Every thread of the block runs the
+// same iterations (the barriers are uniform).
+template <class PR, int TY>
+__device__ __forceinline__ void sweep_tile(const StepPtrs& X, const Geom& G, const Phys& P, int write_macro, int4 t,
+                                           float4* A, float4* B)
+{
+    constexpr int RW = kSweepX + 2, PLANE = (TY + 2) * RW;
+    const int b = t.x & 1;
+    const int x0 = t.y & 0xffff, y0 = t.y >> 16, z0 = t.z & 0xffff, z1 = t.z >> 16;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int nx = box_nx(G, b), ny = box_ny(G, b);
+    const int x = x0 + tx, y = y0 + ty;
+    const float4* __restrict__ M = X.mprev;
+    auto stage = [&](int kk) {
+        const int slot = (kk & 3) * PLANE;
+        for (int e = threadIdx.x; e < PLANE; e += kSweepX * TY) {
+            const int ry = e / RW, rx = e - ry * RW;
+            const int n = tile_rec_node(G, b, x0 + rx - 1, y0 + ry - 1, kk);
+            if (n >= 0) {
+                cp_async16(A + slot + e, M + 2 * (long long)n);
+                cp_async16(B + slot + e, M + 2 * (long long)n + 1);
+            }
+        }
+    };
+    stage(z0 - 1);
+    stage(z0);
+    stage(z0 + 1);
+    cp_async_commit();
+    cp_async_wait_all();
+    __syncthreads();
+    for (int k = z0; k < z1; k++) {
+        // plane k + 2 goes to the slot of plane k - 2, which no thread reads
+        // any more (the barrier at the end of the previous iteration)
+        if (k + 2 < z1 + 1) stage(k + 2);
+        cp_async_commit();
+        if (x < nx && y < ny && !is_boundary(G, b, x + 1, y + 1, k))
+            lp_interior<PR>(X, G, P, write_macro, box_base(G, b) + ((k - 1) * ny + y) * nx + x, b, x + 1, y + 1, k,
+                            RecShared<TY>{A, B, tx, ty, k});
+        cp_async_wait_all();
+        __syncthreads();
     }
 }
 
@@ -1443,6 +1579,44 @@ __device__ __forceinline__ void bulk_any(const StepPtrs& X, const Geom& G, const
     {                                                                                                           \
         for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < G.nnodes; g += gridDim.x * blockDim.x)          \
             bulk_any<PR>(X, G, P, write_macro, g);                                                              \
+    }
+
+// The FP16 form's interior as tiles (sweep_tile): 32 x 8 threads (two blocks
+// per SM) or 32 x 4 (four), persistent over the tile list.
+#define TMX_DEFINE_SWEEP_KERNELS(PR, NAME)                                                                        \
+    __global__ void __launch_bounds__(256, 2) k_sweep8_##NAME(StepPtrs X, Geom G, Phys P, int write_macro,      \
+                                                              const int4* __restrict__ tiles, int ntiles)       \
+    {                                                                                                           \
+        __shared__ float4 A[4 * 10 * (kSweepX + 2)], B[4 * 10 * (kSweepX + 2)];                                 \
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x) sweep_tile<PR, 8>(X, G, P, write_macro, tiles[t], A, B); \
+    }                                                                                                           \
+    __global__ void __launch_bounds__(128, 4) k_sweep4_##NAME(StepPtrs X, Geom G, Phys P, int write_macro,      \
+                                                              const int4* __restrict__ tiles, int ntiles)       \
+    {                                                                                                           \
+        __shared__ float4 A[4 * 6 * (kSweepX + 2)], B[4 * 6 * (kSweepX + 2)];                                   \
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x) sweep_tile<PR, 4>(X, G, P, write_macro, tiles[t], A, B); \
+    }                                                                                                           \
+    __global__ void __launch_bounds__(256, 2) k_sweep_batch8_##NAME(const MixerDesc* __restrict__ D,            \
+        const int4* __restrict__ tiles, const int* __restrict__ counts, int parity, int write_macro)            \
+    {                                                                                                           \
+        __shared__ float4 A[4 * 10 * (kSweepX + 2)], B[4 * 10 * (kSweepX + 2)];                                 \
+        const int n = counts[3];                                                                                \
+        for (int t = blockIdx.x; t < n; t += gridDim.x) {                                                       \
+            const int4 tl = tiles[t];                                                                           \
+            const MixerDesc& d = D[tl.x >> 1];                                                                  \
+            sweep_tile<PR, 8>(d.X[parity], d.G, d.P, write_macro, tl, A, B);                                    \
+        }                                                                                                       \
+    }                                                                                                           \
+    __global__ void __launch_bounds__(128, 4) k_sweep_batch4_##NAME(const MixerDesc* __restrict__ D,            \
+        const int4* __restrict__ tiles, const int* __restrict__ counts, int parity, int write_macro)            \
+    {                                                                                                           \
+        __shared__ float4 A[4 * 6 * (kSweepX + 2)], B[4 * 6 * (kSweepX + 2)];                                   \
+        const int n = counts[3];                                                                                \
+        for (int t = blockIdx.x; t < n; t += gridDim.x) {                                                       \
+            const int4 tl = tiles[t];                                                                           \
+            const MixerDesc& d = D[tl.x >> 1];                                                                  \
+            sweep_tile<PR, 4>(d.X[parity], d.G, d.P, write_macro, tl, A, B);                                    \
+        }                                                                                                       \
     }
 
 // The face and the edge list as two launches (the FP32 and FP16-storage steps;

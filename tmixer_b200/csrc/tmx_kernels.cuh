@@ -76,6 +76,17 @@ TMX_DECLARE_BATCH_KERNELS(f64)
 TMX_DECLARE_BATCH_KERNELS(f32)
 TMX_DECLARE_BATCH_KERNELS(f16)
 
+// The FP16 form's interior by tiles of 32 x TY nodes swept through z
+// (tmx_engine.cuh sweep_tile): tiles[t] = {mixer * 2 + box, x0 | y0 << 16,
+// z0 | z1 << 16}; the single-mixer kernels take mixer 0, the batched ones read
+// the tile count from counts[3].
+__global__ void k_sweep8_f16(StepPtrs X, Geom G, Phys P, int write_macro, const int4* tiles, int ntiles);
+__global__ void k_sweep4_f16(StepPtrs X, Geom G, Phys P, int write_macro, const int4* tiles, int ntiles);
+__global__ void k_sweep_batch8_f16(const MixerDesc* D, const int4* tiles, const int* counts, int parity,
+                                   int write_macro);
+__global__ void k_sweep_batch4_f16(const MixerDesc* D, const int4* tiles, const int* counts, int parity,
+                                   int write_macro);
+
 // Outlet mixing quality of batch mixers: for entry e, mixer slots[e], the
 // I_A, I_B, I_C of mixing row 1 (the first row of tmx_mixing) into
 // out[3e..3e+2], with the arithmetic of k_mixing_rows and its finish.

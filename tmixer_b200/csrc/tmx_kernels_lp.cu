@@ -14,5 +14,6 @@ TMX_DEFINE_BATCH_KERNELS(F32, f32)
 TMX_DEFINE_STEP_KERNELS(F16, f16)
 TMX_DEFINE_BOUNDARY_KERNELS(F16, f16)
 TMX_DEFINE_BATCH_KERNELS(F16, f16)
+TMX_DEFINE_SWEEP_KERNELS(F16, f16)
 
 }  // namespace tmx
