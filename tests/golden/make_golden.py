@@ -60,7 +60,8 @@ def digest_run(name: str, params: dict, steps: int, out_name: str, extra: dict |
     """Run the reference for ``steps`` steps and write the digests of its
     fields and mixing rows to tests/golden/<out_name>."""
     binary = build_ref.build(name, params)
-    dump, mix, secs = oracle.run_ref(binary, steps, threads=os.cpu_count())
+    threads = int(os.environ.get("TMX_GOLDEN_THREADS", os.cpu_count() or 1))
+    dump, mix, secs = oracle.run_ref(binary, steps, threads=threads)
     out = {"steps": steps, "fields": {"b%d_%s" % (b, f): digest(dump[(b, f)]) for b in (0, 1)
                                       for f in oracle.FIELDS},
            "mixing": digest(mix), "mixing_rows": int(mix.shape[0])}
