@@ -98,7 +98,7 @@ def test_tune_restarts_mixers(gpu):
     with T.Batch(T.TMX_FP16, budget=1 << 28) as B:
         slots = [B.add(s) for s in specs]
         best = B.tune(steps_per_trial=3)
-        assert best["kernel"] in ("flat", "sweep8", "sweep4", "sweep8w", "sweep4w")
+        assert best["kernel"] in ("flat", "sweep8", "sweep4")
         assert best["threads"] in (128, 256, 512) and best["cells"] % best["threads"] == 0
         shape = B.shape()
         assert all(shape[k] == best[k] for k in ("kernel", "threads", "cells", "zchunk"))
@@ -124,14 +124,13 @@ def test_wrong_precision_rejected(gpu):
             B.add(_specs(T.TMX_FP32)[0])
 
 
-@pytest.mark.parametrize("tile_y,zchunk,walls", [(8, 3, False), (4, 1, False), (8, 64, False), (8, 4, True),
-                                                 (4, 64, True)])
-def test_sweep_shapes_agree(gpu, tile_y, zchunk, walls):
+@pytest.mark.parametrize("tile_y,zchunk", [(8, 3), (4, 1), (8, 64)])
+def test_sweep_shapes_agree(gpu, tile_y, zchunk):
     """The FP16 form's sweep interior kernel in a batch (tiles of every mixer
     in one list) gives each mixer its solo run's bits."""
     specs = _specs(T.TMX_FP16)
     with T.Batch(T.TMX_FP16, budget=1 << 28) as B:
-        B.set_sweep(tile_y, zchunk, walls)
+        B.set_sweep(tile_y, zchunk)
         slots = [B.add(s) for s in specs]
         B.step(6)
         late = B.add(specs[1])
@@ -139,6 +138,6 @@ def test_sweep_shapes_agree(gpu, tile_y, zchunk, walls):
         for slot, spec in zip(slots, specs):
             _same(B, slot, _alone(spec, 11), 11)
         _same(B, late, _alone(specs[1], 5), 5)
-        assert B.shape()["kernel"] == "sweep%d%s" % (tile_y, "w" if walls else "")
+        assert B.shape()["kernel"] == "sweep%d" % tile_y
         B.set_shape(256, 4096)
         assert B.shape()["kernel"] == "flat"

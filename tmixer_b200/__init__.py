@@ -145,7 +145,7 @@ def lib() -> ctypes.CDLL:
     L.tmx_batch_set_shape.argtypes = [vp, ip, ip]
     L.tmx_batch_tune.argtypes = [vp, ip, P(ip), P(ip), P(dp)]
     L.tmx_batch_time_steps.argtypes = [vp, ip, P(dp)]
-    L.tmx_batch_set_sweep.argtypes = [vp, ip, ip, ip]
+    L.tmx_batch_set_sweep.argtypes = [vp, ip, ip]
     L.tmx_batch_shape.argtypes = [vp, P(ip)]
     L.tmx_batch_checkpoint_size.argtypes = [vp, ip, P(LL)]
     L.tmx_batch_checkpoint.argtypes = [vp, ip, vp, LL]
@@ -391,8 +391,7 @@ class Solver:
     def set_shape(self, kind: int, zchunk: int = 8) -> "Solver":
         """Launch shape of the interior kernel (tmx_set_shape): SHAPE_FLAT, or
         for the FP16 form SHAPE_SWEEP8 / SHAPE_SWEEP4 with zchunk planes per
-        tile (SHAPE_SWEEP8W / SHAPE_SWEEP4W: the tiles also update the wall
-        faces).  Every shape gives the same bits."""
+        tile.  Every shape gives the same bits."""
         _check(lib().tmx_set_shape(self._h, int(kind), int(zchunk)))
         return self
 
@@ -500,26 +499,24 @@ class Batch:
         """The flat interior kernel with this block size and cell-block size."""
         _check(lib().tmx_batch_set_shape(self._b, int(threads), int(cells)))
 
-    def set_sweep(self, tile_y: int, zchunk: int, walls: bool = False) -> None:
+    def set_sweep(self, tile_y: int, zchunk: int) -> None:
         """The FP16 form's sweep interior kernel: tiles of 32 x tile_y nodes
-        walked through zchunk planes; walls: the tiles also update the wall
-        faces."""
-        _check(lib().tmx_batch_set_sweep(self._b, int(tile_y), int(zchunk), int(bool(walls))))
+        walked through zchunk planes."""
+        _check(lib().tmx_batch_set_sweep(self._b, int(tile_y), int(zchunk)))
 
     def shape(self) -> dict:
         o = (ctypes.c_int * 4)()
         _check(lib().tmx_batch_shape(self._b, o))
-        return dict(kernel=SHAPE_NAMES[o[0]], threads=o[1], cells=o[2], zchunk=o[3],
-                    nodes_per_thread=(o[2] // o[1]) if o[0] == SHAPE_FLAT else o[3],
-                    wall_faces="face kernel" if o[0] in (SHAPE_FLAT, SHAPE_SWEEP8, SHAPE_SWEEP4) else "tiles")
+        kind = {SHAPE_FLAT: "flat", SHAPE_SWEEP8: "sweep8", SHAPE_SWEEP4: "sweep4"}[o[0]]
+        return dict(kernel=kind, threads=o[1], cells=o[2], zchunk=o[3],
+                    nodes_per_thread=(o[2] // o[1]) if o[0] == SHAPE_FLAT else o[3])
 
     def set_from(self, shape: dict) -> None:
         """Apply a shape() dictionary (e.g. the tuned shape of another batch)."""
         if shape["kernel"] == "flat":
             self.set_shape(shape["threads"], shape["cells"])
         else:
-            self.set_sweep(8 if shape["kernel"].startswith("sweep8") else 4, shape["zchunk"],
-                           shape["kernel"].endswith("w"))
+            self.set_sweep(8 if shape["kernel"] == "sweep8" else 4, shape["zchunk"])
 
     def tune(self, steps_per_trial: int = 20) -> dict:
         """Autotune the interior kernel's shape (tmx_batch_tune) and return it
@@ -567,9 +564,7 @@ class Request:
                          float(self.tol))
 
 
-SHAPE_FLAT, SHAPE_SWEEP8, SHAPE_SWEEP4, SHAPE_SWEEP8W, SHAPE_SWEEP4W = 0, 1, 2, 3, 4
-SHAPE_NAMES = {SHAPE_FLAT: "flat", SHAPE_SWEEP8: "sweep8", SHAPE_SWEEP4: "sweep4", SHAPE_SWEEP8W: "sweep8w",
-               SHAPE_SWEEP4W: "sweep4w"}
+SHAPE_FLAT, SHAPE_SWEEP8, SHAPE_SWEEP4 = 0, 1, 2
 
 SERVE_STATUS = {0: "converged", 1: "max_steps", -2: "too large for the budget", -5: "non-finite"}
 
@@ -665,5 +660,5 @@ def serve_with(engine, requests, check_every: int = 100, max_active: int = 0):
     return _serve_out(reqs, res[:len(reqs)], summ)
 
 
-__all__ = ["SHAPE_FLAT", "SHAPE_SWEEP8", "SHAPE_SWEEP4", "SHAPE_SWEEP8W", "SHAPE_SWEEP4W", "CaseSpec", "Solver", "Batch", "Request", "serve", "serve_with", "TmxError", "FIELDS", "TMX_FP64", "TMX_FP32", "TMX_FP16", "PRECISIONS",
+__all__ = ["SHAPE_FLAT", "SHAPE_SWEEP8", "SHAPE_SWEEP4", "CaseSpec", "Solver", "Batch", "Request", "serve", "serve_with", "TmxError", "FIELDS", "TMX_FP64", "TMX_FP32", "TMX_FP16", "PRECISIONS",
            "reference_case", "w_layout", "lib"]

@@ -75,7 +75,6 @@ struct tmx_handle {
     cudaStream_t aux = nullptr, aux2 = nullptr;
     cudaEvent_t fork = nullptr, join = nullptr, join2 = nullptr;
     int nface = 0;  // the first nface boundary nodes are face classes
-    int nface_open = 0;  // the first nface_open of them are not wall faces
     int nwall = 0;  // the last nwall are wall faces (StepKernels::walls)
     // one captured step per (state buffer, macroscopic output) combination
     cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
@@ -350,11 +349,9 @@ int boundary_list(const Geom& G, std::vector<int>& nodes, std::vector<unsigned c
                         return fail(TMX_E_INVALID, "internal: wall class %d of node (%d,%d,%d,%d), class %d", w, b, i,
                                     j, k, c);
                     if (class_count) (*class_count)[c]++;
-                    // faces first (the wall faces after the others), then
-                    // edges and corners (or, with nwall, the wall faces last);
-                    // by class, then node
-                    const int key = (nwall && w >= 0) ? 512
-                                                      : (tmx::is_face_class(c) ? (w >= 0 ? 128 : 0) : 256) + c;
+                    // faces first, then edges and corners (then, with nwall,
+                    // the wall faces); by class, then node
+                    const int key = (nwall && w >= 0) ? 512 : (tmx::is_face_class(c) ? 0 : 256) + c;
                     bl.emplace_back(key, tmx::node_index(G, b, i, j, k));
                 }
     std::sort(bl.begin(), bl.end());
@@ -443,9 +440,7 @@ int enqueue_step(tmx_handle* h, int cur, int write_macro, cudaEvent_t* ev)
     TMX_CK(cudaStreamWaitEvent(h->aux, h->fork, 0));
     TMX_CK(cudaStreamWaitEvent(h->aux2, h->fork, 0));
     if (ev) TMX_CK(cudaEventRecord(ev[2], h->aux));
-    // the sweep shapes with walls update the wall faces themselves
-    const bool tile_walls = h->shape == TMX_SHAPE_SWEEP8W || h->shape == TMX_SHAPE_SWEEP4W;
-    const int nf = tile_walls ? h->nface_open : h->nface, nw = h->nwall, ne = h->nb - h->nface - h->nwall;
+    const int nf = h->nface, nw = h->nwall, ne = h->nb - h->nface - h->nwall;
     const int bt = tmx::kBoundaryThreadsHost, nl = tmx::kBoundaryLanesHost;  // nl threads per node
     if (h->K->serial) {
         // one launch, the edge and corner blocks first: their long per-node
@@ -461,8 +456,8 @@ int enqueue_step(tmx_handle* h, int cur, int write_macro, cudaEvent_t* ev)
         if (nf > 0)
             h->K->faces<<<(nl * nf + bt - 1) / bt, bt, 0, h->aux>>>(X, h->bnode, h->bcls, nf, G, h->P, write_macro);
         if (ne > 0)
-            h->K->edges<<<(nl * ne + bt - 1) / bt, bt, 0, h->aux2>>>(X, h->bnode + h->nface, h->bcls + h->nface, ne,
-                                                                     G, h->P, write_macro);
+            h->K->edges<<<(nl * ne + bt - 1) / bt, bt, 0, h->aux2>>>(X, h->bnode + nf, h->bcls + nf, ne, G, h->P,
+                                                                     write_macro);
     }
     TMX_CK(cudaEventRecord(h->join2, h->aux2));
     if (ev) {  // the boundary time spans both boundary kernels
@@ -481,9 +476,9 @@ int enqueue_step(tmx_handle* h, int cur, int write_macro, cudaEvent_t* ev)
         TMX_CK(cudaStreamWaitEvent(h->stream, h->join2, 0));
     }
     if (ev) TMX_CK(cudaEventRecord(ev[0], h->stream));
-    if (h->shape == TMX_SHAPE_SWEEP8 || h->shape == TMX_SHAPE_SWEEP8W)
+    if (h->shape == TMX_SHAPE_SWEEP8)
         tmx::k_sweep8_f16<<<h->sweep_blocks, 256, 0, h->stream>>>(X, G, h->P, write_macro, h->tiles, h->ntiles);
-    else if (h->shape == TMX_SHAPE_SWEEP4 || h->shape == TMX_SHAPE_SWEEP4W)
+    else if (h->shape == TMX_SHAPE_SWEEP4)
         tmx::k_sweep4_f16<<<h->sweep_blocks, 128, 0, h->stream>>>(X, G, h->P, write_macro, h->tiles, h->ntiles);
     else
         h->K->bulk<<<h->bulk_blocks, 256, 0, h->stream>>>(X, G, h->P, write_macro);
@@ -704,7 +699,6 @@ int tmx_create(const tmx_case* c, int device, tmx_handle** out)
         return rc;
     }
     h->nb = (int)nodes.size();
-    while (h->nface_open < h->nface && !tmx::is_wall_class(cls[h->nface_open])) h->nface_open++;
 
     auto alloc = [&](void** p, size_t n) -> cudaError_t {
         cudaError_t e = cudaMalloc(p, n);
@@ -748,7 +742,7 @@ int tmx_create(const tmx_case* c, int device, tmx_handle** out)
 int tmx_set_shape(tmx_handle* h, int kind, int zchunk)
 {
     if (!h) return fail(TMX_E_INVALID, "null handle");
-    if (kind < TMX_SHAPE_FLAT || kind > TMX_SHAPE_SWEEP4W)
+    if (kind != TMX_SHAPE_FLAT && kind != TMX_SHAPE_SWEEP8 && kind != TMX_SHAPE_SWEEP4)
         return fail(TMX_E_INVALID, "tmx_set_shape: unknown kind %d", kind);
     if (kind != TMX_SHAPE_FLAT && !h->K->moments)
         return fail(TMX_E_INVALID, "tmx_set_shape: the sweep shapes are for the FP16 form only");
@@ -756,10 +750,9 @@ int tmx_set_shape(tmx_handle* h, int kind, int zchunk)
     TMX_CK(cudaSetDevice(h->device));
     TMX_CK(cudaStreamSynchronize(h->stream));
     if (kind != TMX_SHAPE_FLAT) {
-        const int ty = (kind == TMX_SHAPE_SWEEP8 || kind == TMX_SHAPE_SWEEP8W) ? 8 : 4;
-        const int walls = (kind == TMX_SHAPE_SWEEP8W || kind == TMX_SHAPE_SWEEP4W) ? 1 : 0;
+        const int ty = kind == TMX_SHAPE_SWEEP8 ? 8 : 4;
         std::vector<int4> t;
-        sweep_tiles(h->G, 0, ty, zchunk, walls, t);
+        sweep_tiles(h->G, 0, ty, zchunk, t);
         int4* d = nullptr;
         if (!t.empty()) {
             cudaError_t e = cudaMalloc((void**)&d, t.size() * sizeof(int4));

@@ -217,7 +217,6 @@ struct tmx_batch {
     int cells = 4096;    // nodes per cell block
     int sweep = 0;       // 0: the flat kernel; 8 or 4: the sweep kernel of that tile height
     int zchunk = 8;      // planes per sweep tile
-    int sweep_walls = 0; // 1: the sweep tiles update the wall faces, the face list leaves them out
     int sms = 148;
     int grid_bulk[3] = {0, 0, 0};
     int grid_sweep[2] = {0, 0};  // tile height 8, 4
@@ -297,15 +296,13 @@ int rebuild(tmx_batch* b)
         desc[m] = desc_of(b, s);
         for (int g0 = 0; g0 < s.G.nnodes; g0 += b->cells)
             blocks.push_back(make_int4((int)m, g0, std::min(b->cells, s.G.nnodes - g0), 0));
-        const bool tile_walls = b->sweep && b->sweep_walls;
-        if (b->sweep) sweep_tiles(s.G, (int)m, b->sweep, b->zchunk, tile_walls ? 1 : 0, tiles);
+        if (b->sweep) sweep_tiles(s.G, (int)m, b->sweep, b->zchunk, tiles);
         for (size_t t = 0; t < s.nodes.size(); t++) {
             const int2 e = make_int2(s.nodes[t], (int)m * 256 + s.cls[t]);
-            if ((int)t < s.nface) {
-                if (!(tile_walls && tmx::is_wall_class(s.cls[t]))) faces.push_back(e);
-            } else {
+            if ((int)t < s.nface)
+                faces.push_back(e);
+            else
                 edges.push_back(e);
-            }
         }
     }
     cudaError_t e = grow(b, b->d_desc, b->cap_desc, (int)std::max<size_t>(1, desc.size()));
@@ -833,7 +830,7 @@ int tmx_batch_set_shape(tmx_batch* b, int threads, int cells)
     return TMX_OK;
 }
 
-int tmx_batch_set_sweep(tmx_batch* b, int tile_y, int zchunk, int walls)
+int tmx_batch_set_sweep(tmx_batch* b, int tile_y, int zchunk)
 {
     if (!b) return fail(TMX_E_INVALID, "null batch");
     if (tile_y != 8 && tile_y != 4) return fail(TMX_E_INVALID, "sweep tile height must be 8 or 4 (got %d)", tile_y);
@@ -842,18 +839,16 @@ int tmx_batch_set_sweep(tmx_batch* b, int tile_y, int zchunk, int walls)
     TMX_CK(cudaSetDevice(b->device));
     TMX_CK(cudaStreamSynchronize(b->stream));
     if (tile_y != b->sweep) drop_graphs(b);
-    if (tile_y != b->sweep || zchunk != b->zchunk || (walls != 0) != (b->sweep_walls != 0)) b->dirty = true;
+    if (tile_y != b->sweep || zchunk != b->zchunk) b->dirty = true;
     b->sweep = tile_y;
     b->zchunk = zchunk;
-    b->sweep_walls = walls ? 1 : 0;
     return TMX_OK;
 }
 
 int tmx_batch_shape(const tmx_batch* b, int out[4])
 {
     if (!b || !out) return fail(TMX_E_INVALID, "null argument");
-    out[0] = b->sweep == 8 ? (b->sweep_walls ? TMX_SHAPE_SWEEP8W : TMX_SHAPE_SWEEP8)
-                           : (b->sweep == 4 ? (b->sweep_walls ? TMX_SHAPE_SWEEP4W : TMX_SHAPE_SWEEP4) : TMX_SHAPE_FLAT);
+    out[0] = b->sweep == 8 ? TMX_SHAPE_SWEEP8 : (b->sweep == 4 ? TMX_SHAPE_SWEEP4 : TMX_SHAPE_FLAT);
     out[1] = b->sweep ? 32 * b->sweep : kBulkThreads[b->variant];
     out[2] = b->cells;
     out[3] = b->zchunk;
@@ -872,7 +867,7 @@ int tmx_batch_tune(tmx_batch* b, int steps_per_trial, int* threads_out, int* cel
     TMX_CK(cudaEventCreate(&t0));
     TMX_CK(cudaEventCreate(&t1));
     double best = 1e300;
-    int bv = b->variant, bc = b->cells, bs = b->sweep, bz = b->zchunk, bw = b->sweep_walls;
+    int bv = b->variant, bc = b->cells, bs = b->sweep, bz = b->zchunk;
     int rc = TMX_OK;
     // time steps_per_trial steps of the shape just set (after two steps that
     // capture its graphs and warm up)
@@ -903,25 +898,23 @@ int tmx_batch_tune(tmx_batch* b, int steps_per_trial, int* threads_out, int* cel
             }
         }
     if (b->K->moments)
-        for (int walls : {0, 1})
-            for (int ty : {8, 4})
-                for (int zi = 0; zi < 4 && rc == TMX_OK; zi++) {
-                    rc = tmx_batch_set_sweep(b, ty, kZChunkChoices[zi], walls);
-                    if (rc) break;
-                    double ms = 0;
-                    trial(ms);
-                    if (rc == TMX_OK && ms < best) {
-                        best = ms;
-                        bs = ty;
-                        bz = kZChunkChoices[zi];
-                        bw = walls;
-                    }
+        for (int ty : {8, 4})
+            for (int zi = 0; zi < 4 && rc == TMX_OK; zi++) {
+                rc = tmx_batch_set_sweep(b, ty, kZChunkChoices[zi]);
+                if (rc) break;
+                double ms = 0;
+                trial(ms);
+                if (rc == TMX_OK && ms < best) {
+                    best = ms;
+                    bs = ty;
+                    bz = kZChunkChoices[zi];
                 }
+            }
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
     if (rc) return rc;
     rc = tmx_batch_set_shape(b, kBulkThreads[bv], bc);
-    if (rc == TMX_OK && bs) rc = tmx_batch_set_sweep(b, bs, bz, bw);
+    if (rc == TMX_OK && bs) rc = tmx_batch_set_sweep(b, bs, bz);
     if (rc) return rc;
     // the trials advanced the mixers: start every one of them again
     TMX_CK(cudaStreamSynchronize(b->stream));

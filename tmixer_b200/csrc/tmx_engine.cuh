@@ -674,6 +674,93 @@ __device__ __forceinline__ void bulk_node_lp(const StepPtrs& X, const Geom& G, c
 }
 
 // ---------------------------------------------------------------------------
+// FP16 form, interior nodes by tiles (the sweep kernels).  A block of 32 x TY
+// threads owns a tile of 32 x TY nodes of one box (x0.., y0..) and walks it
+// through the planes z0 .. z1-1, one node per thread per plane.  The writer
+// records its nodes read (the 9 source rows of each node, 19 reads per node in
+// the flat kernel) are staged once per plane in shared memory: a ring of four
+// planes of (TY + 2) x 34 records (the tile and a one-node halo), the next
+// plane but one copied asynchronously (cp.async) while the current plane is
+// computed.  The populations stream straight from global memory.  Each node's
+// arithmetic is lp_interior's, so the results are the flat kernel's bit for
+// bit.
+// ---------------------------------------------------------------------------
+constexpr int kSweepX = 32;
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
+{
+    const unsigned a = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(a), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// The node whose record a tile of box b stages at 0-based (x, y) of plane kk:
+// the node itself inside the box; on the inlet box's row y = -1 over the
+// opening the mixing box's row mny, and on the mixing box's row y = mny the
+// inlet box's row 1 (the sources of the two interface rules, as bulk_src);
+// -1 where there is no node.
+__device__ __forceinline__ int tile_rec_node(const Geom& G, int b, int x, int y, int kk)
+{
+    if (kk < 1 || kk > G.nz) return -1;
+    const int nx = box_nx(G, b), ny = box_ny(G, b);
+    if (x >= 0 && x < nx && y >= 0 && y < ny) return box_base(G, b) + ((kk - 1) * ny + y) * nx + x;
+    if (b == 0 && y == -1) {
+        const int xm = x - (G.ia - 1);
+        if (xm >= 0 && xm < G.mnx) return G.base[1] + ((kk - 1) * G.mny + (G.mny - 1)) * G.mnx + xm;
+    } else if (b == 1 && y == G.mny) {
+        const int xi = x + G.ia - 1;
+        if (xi >= 0 && xi < G.inx) return ((kk - 1) * G.iny) * G.inx + xi;
+    }
+    return -1;
+}
+
+// One tile {mixer * 2 + box, x0 | y0 << 16, z0 | z1 << 16} (0-based x0, y0;
+// interior planes z0 .. z1-1, 2 <= z0 < z1 <= nz).  A and B hold the two
+// halves of 4 * (TY + 2) * 34 records.  Every thread of the block runs the
+// same iterations (the barriers are uniform).
+template <class PR, int TY>
+__device__ __forceinline__ void sweep_tile(const StepPtrs& X, const Geom& G, const Phys& P, int write_macro, int4 t,
+                                           float4* A, float4* B)
+{
+    constexpr int RW = kSweepX + 2, PLANE = (TY + 2) * RW;
+    const int b = t.x & 1;
+    const int x0 = t.y & 0xffff, y0 = t.y >> 16, z0 = t.z & 0xffff, z1 = t.z >> 16;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int nx = box_nx(G, b), ny = box_ny(G, b);
+    const int x = x0 + tx, y = y0 + ty;
+    const float4* __restrict__ M = X.mprev;
+    auto stage = [&](int kk) {
+        const int slot = (kk & 3) * PLANE;
+        for (int e = threadIdx.x; e < PLANE; e += kSweepX * TY) {
+            const int ry = e / RW, rx = e - ry * RW;
+            const int n = tile_rec_node(G, b, x0 + rx - 1, y0 + ry - 1, kk);
+            if (n >= 0) {
+                cp_async16(A + slot + e, M + 2 * (long long)n);
+                cp_async16(B + slot + e, M + 2 * (long long)n + 1);
+            }
+        }
+    };
+    stage(z0 - 1);
+    stage(z0);
+    stage(z0 + 1);
+    cp_async_commit();
+    cp_async_wait_all();
+    __syncthreads();
+    for (int k = z0; k < z1; k++) {
+        // plane k + 2 goes to the slot of plane k - 2, which no thread reads
+        // any more (the barrier at the end of the previous iteration)
+        if (k + 2 < z1 + 1) stage(k + 2);
+        cp_async_commit();
+        if (x < nx && y < ny && !is_boundary(G, b, x + 1, y + 1, k))
+            lp_interior<PR>(X, G, P, write_macro, box_base(G, b) + ((k - 1) * ny + y) * nx + x, b, x + 1, y + 1, k,
+                            RecShared<TY>{A, B, tx, ty, k});
+        cp_async_wait_all();
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
 // boundary closures (Tmixer.cpp:2023-9033)
 // ---------------------------------------------------------------------------
 template <class PR>
@@ -1122,202 +1209,6 @@ __device__ __forceinline__ void face_copy_offset(int cls, int& di, int& dj, int&
     case K_FACE_Z1: dk = 1; break;
     default: break;
     }
-}
-
-// One wall face node (tmx::wall_class: the z = 1 and z = nz planes, the inlet
-// box's y walls, the outlet row) of a reduced-precision form in one thread:
-// the flow pulled from its own sources (ghost sources 0) and closed, the
-// species a copy of the interior neighbour's pulled values, then the
-// moments and the collision.  Every value is computed with the operations, in
-// the order, of the four-lane face kernel (boundary_lane_lp: decode_pairs,
-// wall_flow_closure, sums in index order, the outlet's pinned density,
-// collide_pairs), so the two give the same bits.  Not inlined: the sweep
-// kernels call it for their wall rows and planes and keep their interior
-// path's registers.
-template <class PR>
-__device__ __noinline__ void lp_wall(const StepPtrs& X, const Geom& G, const Phys& P, int write_macro, int g, int b,
-                                     int i, int j, int k, int cls)
-{
-    using T = typename PR::T;
-    const typename PR::S* __restrict__ Pin = (const typename PR::S*)X.pin;
-    typename PR::S* __restrict__ Pout = (typename PR::S*)X.pout;
-    const float4* __restrict__ M = X.mprev;
-    const long long ps = G.ps;
-    int di, dj, dk;
-    face_copy_offset(cls, di, dj, dk);
-    T f[19];
-    float2 p01[19], p23[19];
-#pragma unroll
-    for (int q = 0; q < 19; q++) {
-        const int s0 = pull_src_e(G, b, i, j, k, EX(q), EY(q), EZ(q));
-        const int s1 = pull_src_e(G, b, i + di, j + dj, k + dk, EX(q), EY(q), EZ(q));
-        float4 mf = make_float4(0.f, 0.f, 0.f, 0.f), ms = mf;
-        float2 a01 = make_float2(0.f, 0.f), a23 = a01;
-        if (s0 >= 0) {
-            if constexpr (PR::kMoments) RecGlobal{M}(q, s0, mf, ms);
-            PR::decode_pairs_rec(Pin, ps, q, EX(q), EY(q), EZ(q), (float)wq(q), s0, mf, ms, a01, a23);
-        }
-        f[q] = a01.x;
-        a01 = make_float2(0.f, 0.f);
-        a23 = a01;
-        if (s1 >= 0) {
-            if constexpr (PR::kMoments) RecGlobal{M}(q, s1, mf, ms);
-            PR::decode_pairs_rec(Pin, ps, q, EX(q), EY(q), EZ(q), (float)wq(q), s1, mf, ms, a01, a23);
-        }
-        p01[q] = a01;
-        p23[q] = a23;
-    }
-    wall_flow_closure(cls, T(P.rho_out), f);
-#pragma unroll
-    for (int q = 0; q < 19; q++) p01[q].x = f[q];
-    float2 s01 = p01[0], s23 = p23[0];
-#pragma unroll
-    for (int q = 1; q < 19; q++) {
-        s01 = __fadd2_rn(s01, p01[q]);
-        s23 = __fadd2_rn(s23, p23[q]);
-    }
-    T rho = s01.x;
-    const T ca = s01.y, cb = s23.x, cc = s23.y;
-    // the outlet row's density is pinned to rho_out (Tmixer.cpp:9575-9582)
-    if (b == 1 && j == 1) rho = T(P.rho_out);
-    T sxm, sym, szm;
-    momentum(f, sxm, sym, szm);
-    const T ux = sxm / rho, uy = sym / rho, uz = szm / rho;
-    T poly[19];
-    PR::poly(ux, uy, uz, poly);
-    const T rt = T(P.rateconst) * ca * cb;
-    const float2 r01 = make_float2(rho, ca), r23 = make_float2(cb, cc);
-    const float2 c1a = make_float2((float)P.c1[0], (float)P.c1[1]), c1b = make_float2((float)P.c1[2], (float)P.c1[3]);
-    const float2 c2a = make_float2((float)P.c2[0], (float)P.c2[1]), c2b = make_float2((float)P.c2[2], (float)P.c2[3]);
-#pragma unroll
-    for (int q = 0; q < 19; q++) {
-        float2 o01, o23, f01, f23;
-        collide_pairs(p01[q], p23[q], r01, r23, poly[q], c1a, c1b, c2a, c2b, (float)wq(q) * rt, o01, o23, f01, f23);
-        PR::store_pairs(Pout, q, ps, g, o01, o23, f01, f23);
-    }
-    T* __restrict__ Rcur = (T*)X.rcur;
-    Rcur[g] = rho;
-    Rcur[ps + g] = ca;
-    Rcur[2 * ps + g] = cb;
-    Rcur[3 * ps + g] = cc;
-    if (PR::kMoments) {
-        X.mcur[2 * (long long)g] = make_float4((float)rho, (float)ux, (float)uy, (float)uz);
-        X.mcur[2 * (long long)g + 1] =
-            make_float4((float)ca, (float)cb, (float)cc, u2_term((float)ux, (float)uy, (float)uz));
-    }
-    if (write_macro) {
-        double* Mac = X.mac;
-        Mac[g] = rho;
-        Mac[ps + g] = ux;
-        Mac[2 * ps + g] = uy;
-        Mac[3 * ps + g] = uz;
-        Mac[4 * ps + g] = ca;
-        Mac[5 * ps + g] = cb;
-        Mac[6 * ps + g] = cc;
-    }
-}
-
-// ---------------------------------------------------------------------------
-// FP16 form, interior nodes by tiles (the sweep kernels).  A block of 32 x TY
-// threads owns a tile of 32 x TY nodes of one box (x0.., y0..) and walks it
-// through the planes z0 .. z1-1, one node per thread per plane.  The writer
-// records its nodes read (the 9 source rows of each node, 19 reads per node in
-// the flat kernel) are staged once per plane in shared memory: a ring of four
-// planes of (TY + 2) x 34 records (the tile and a one-node halo), the next
-// plane but one copied asynchronously (cp.async) while the current plane is
-// computed.  The populations stream straight from global memory.  Each node's
-// arithmetic is lp_interior's, so the results are the flat kernel's bit for
-// bit.
-// ---------------------------------------------------------------------------
-constexpr int kSweepX = 32;
-
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
-{
-    const unsigned a = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(a), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-
-// The node whose record a tile of box b stages at 0-based (x, y) of plane kk:
-// the node itself inside the box; on the inlet box's row y = -1 over the
-// opening the mixing box's row mny, and on the mixing box's row y = mny the
-// inlet box's row 1 (the sources of the two interface rules, as bulk_src);
-// -1 where there is no node.
-__device__ __forceinline__ int tile_rec_node(const Geom& G, int b, int x, int y, int kk)
-{
-    if (kk < 1 || kk > G.nz) return -1;
-    const int nx = box_nx(G, b), ny = box_ny(G, b);
-    if (x >= 0 && x < nx && y >= 0 && y < ny) return box_base(G, b) + ((kk - 1) * ny + y) * nx + x;
-    if (b == 0 && y == -1) {
-        const int xm = x - (G.ia - 1);
-        if (xm >= 0 && xm < G.mnx) return G.base[1] + ((kk - 1) * G.mny + (G.mny - 1)) * G.mnx + xm;
-    } else if (b == 1 && y == G.mny) {
-        const int xi = x + G.ia - 1;
-        if (xi >= 0 && xi < G.inx) return ((kk - 1) * G.iny) * G.inx + xi;
-    }
-    return -1;
-}
-
-// One tile {mixer * 2 + box, x0 | y0 << 16, z0 | z1 << 16, walls} (0-based
-// x0, y0; interior planes z0 .. z1-1, 2 <= z0 < z1 <= nz).  With walls = 1
-// the tile also updates its wall face nodes (lp_wall): those of its rows in
-// the planes it sweeps, and the z = 1 (z = nz) plane when its chunk starts at
-// z = 2 (ends at nz - 1).  A and B hold the two halves of 4 * (TY + 2) * 34
-// records.  Every thread of the block runs the same iterations (the barriers
-// are uniform).
-template <class PR, int TY>
-__device__ __forceinline__ void sweep_tile(const StepPtrs& X, const Geom& G, const Phys& P, int write_macro, int4 t,
-                                           float4* A, float4* B)
-{
-    constexpr int RW = kSweepX + 2, PLANE = (TY + 2) * RW;
-    const int b = t.x & 1;
-    const int x0 = t.y & 0xffff, y0 = t.y >> 16, z0 = t.z & 0xffff, z1 = t.z >> 16;
-    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-    const int nx = box_nx(G, b), ny = box_ny(G, b);
-    const int x = x0 + tx, y = y0 + ty;
-    const float4* __restrict__ M = X.mprev;
-    auto stage = [&](int kk) {
-        const int slot = (kk & 3) * PLANE;
-        for (int e = threadIdx.x; e < PLANE; e += kSweepX * TY) {
-            const int ry = e / RW, rx = e - ry * RW;
-            const int n = tile_rec_node(G, b, x0 + rx - 1, y0 + ry - 1, kk);
-            if (n >= 0) {
-                cp_async16(A + slot + e, M + 2 * (long long)n);
-                cp_async16(B + slot + e, M + 2 * (long long)n + 1);
-            }
-        }
-    };
-    stage(z0 - 1);
-    stage(z0);
-    stage(z0 + 1);
-    cp_async_commit();
-    cp_async_wait_all();
-    __syncthreads();
-    for (int k = z0; k < z1; k++) {
-        // plane k + 2 goes to the slot of plane k - 2, which no thread reads
-        // any more (the barrier at the end of the previous iteration)
-        if (k + 2 < z1 + 1) stage(k + 2);
-        cp_async_commit();
-        if (x < nx && y < ny) {
-            const int g = box_base(G, b) + ((k - 1) * ny + y) * nx + x;
-            const int wc = t.w ? wall_class(G, b, x + 1, y + 1, k) : -1;
-            if (wc >= 0)
-                lp_wall<PR>(X, G, P, write_macro, g, b, x + 1, y + 1, k, wc);
-            else if (!is_boundary(G, b, x + 1, y + 1, k))
-                lp_interior<PR>(X, G, P, write_macro, g, b, x + 1, y + 1, k, RecShared<TY>{A, B, tx, ty, k});
-        }
-        cp_async_wait_all();
-        __syncthreads();
-    }
-    // the z wall planes next to this chunk (their records come from global
-    // memory, so the ring is not involved)
-    if (t.w && x < nx && y < ny)
-        for (int kk : {1, G.nz})
-            if ((kk == 1 && z0 == 2) || (kk == G.nz && z1 == G.nz)) {
-                const int wc = wall_class(G, b, x + 1, y + 1, kk);
-                if (wc >= 0) lp_wall<PR>(X, G, P, write_macro, box_base(G, b) + ((kk - 1) * ny + y) * nx + x, b, x + 1, y + 1, kk, wc);
-            }
 }
 
 template <class PR, bool FACES>

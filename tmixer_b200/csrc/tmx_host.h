@@ -78,17 +78,17 @@ void inlet_scale(const tmx_case& c, const std::vector<double>& raw, double avera
                  std::vector<double>& U2);
 
 // Tiles of the sweep kernels (tmx_engine.cuh sweep_tile) for one mixer:
-// {mixer * 2 + box, x0 | y0 << 16, z0 | z1 << 16, walls}, 32 x ty nodes of a
-// box (0-based x0, y0) over the interior planes z0 .. z1-1 (zchunk at most),
-// z-chunks outermost; walls = 1: the tiles update the wall faces too.
-inline void sweep_tiles(const Geom& G, int mixer, int ty, int zchunk, int walls, std::vector<int4>& out)
+// {mixer * 2 + box, x0 | y0 << 16, z0 | z1 << 16, 0}, 32 x ty nodes of a box
+// (0-based x0, y0) over the interior planes z0 .. z1-1 (zchunk at most),
+// z-chunks outermost.
+inline void sweep_tiles(const Geom& G, int mixer, int ty, int zchunk, std::vector<int4>& out)
 {
     for (int z0 = 2; z0 <= G.nz - 1; z0 += zchunk) {
         const int z1 = z0 + zchunk < G.nz ? z0 + zchunk : G.nz;
         for (int b = 0; b < 2; b++)
             for (int y0 = 0; y0 < G.ny[b]; y0 += ty)
                 for (int x0 = 0; x0 < G.nx[b]; x0 += 32)
-                    out.push_back(make_int4(mixer * 2 + b, x0 | (y0 << 16), z0 | (z1 << 16), walls));
+                    out.push_back(make_int4(mixer * 2 + b, x0 | (y0 << 16), z0 | (z1 << 16), 0));
     }
 }
 
