@@ -241,14 +241,19 @@ int tmx_time_steps(tmx_handle *h, int nsteps, double *ms);
 
 /* Launch shape of the interior (bulk) kernel; no counterpart in the
  * reference.  kind TMX_SHAPE_FLAT: one thread per node over the flat node
- * range (every form; zchunk ignored).  TMX_SHAPE_SWEEP8 / TMX_SHAPE_SWEEP4
- * (FP16 form only): blocks of 32 x 8 (or 32 x 4) threads own tiles of as many
- * nodes of one box and walk them through zchunk planes (zchunk >= 1), the
- * writers' moment records staged in shared memory.  Every shape gives the
- * same results bit for bit.  Default: TMX_SHAPE_FLAT. */
+ * range (every form; zchunk ignored).  The sweep shapes (FP16 form only):
+ * blocks of 32 x TY threads own tiles of as many nodes of one box and walk
+ * them through zchunk planes (zchunk >= 1), the writers' moment records
+ * staged in shared memory: TMX_SHAPE_SWEEP8 (TY 8), TMX_SHAPE_SWEEP4 (TY 4);
+ * TMX_SHAPE_SWEEP4P / TMX_SHAPE_SWEEP2P (TY 4 / 2) also copy each node's
+ * stored populations of the next plane into shared memory while the current
+ * plane is computed.  Every shape gives the same results bit for bit.
+ * Default: TMX_SHAPE_FLAT. */
 #define TMX_SHAPE_FLAT 0
 #define TMX_SHAPE_SWEEP8 1
 #define TMX_SHAPE_SWEEP4 2
+#define TMX_SHAPE_SWEEP4P 3
+#define TMX_SHAPE_SWEEP2P 4
 int tmx_set_shape(tmx_handle *h, int kind, int zchunk);
 
 /* Node counts: out[0] fluid nodes (both boxes), out[1] interior nodes,
@@ -333,21 +338,21 @@ int tmx_batch_set_shape(tmx_batch *b, int threads, int cells);
 
 /* Autotune the launch shape on the batch's current mixers: time
  * steps_per_trial steps of every shape of the interior kernel (the flat
- * kernel's (threads, cells) choices; for the FP16 form also the sweep
- * kernels' tile heights 8 and 4 with 4, 8, 16 or 32 planes per tile, i.e.
- * nodes per thread), keep the fastest, then start every mixer again from its
+ * kernel's (threads, cells) choices; for the FP16 form also every sweep
+ * shape with 4, 8, 16 or 32 planes per tile, i.e. nodes per thread), keep
+ * the fastest, then start every mixer again from its
  * initial state.  Returns the threads per block, the nodes per cell block
  * (flat) or per tile (sweep), and the time per step (ms); tmx_batch_shape
  * tells which kernel won. */
 int tmx_batch_tune(tmx_batch *b, int steps_per_trial, int *threads_out, int *cells_out, double *ms_out);
 
-/* Use the FP16 form's sweep kernel for the interior: tiles of 32 x tile_y
- * nodes (tile_y 8 or 4) walked through zchunk planes (see tmx_set_shape).
+/* Use one of the FP16 form's sweep kernels for the interior: kind a
+ * TMX_SHAPE_SWEEP* shape, zchunk planes per tile (see tmx_set_shape).
  * tmx_batch_set_shape switches back to the flat kernel.  No counterpart in
  * the reference. */
-int tmx_batch_set_sweep(tmx_batch *b, int tile_y, int zchunk);
+int tmx_batch_set_sweep(tmx_batch *b, int kind, int zchunk);
 
-/* The interior kernel's shape: out[0] TMX_SHAPE_FLAT / SWEEP8 / SWEEP4,
+/* The interior kernel's shape: out[0] TMX_SHAPE_*,
  * out[1] threads per block, out[2] nodes per cell block of the flat kernel,
  * out[3] planes per sweep tile. */
 int tmx_batch_shape(const tmx_batch *b, int out[4]);

@@ -98,7 +98,7 @@ def test_tune_restarts_mixers(gpu):
     with T.Batch(T.TMX_FP16, budget=1 << 28) as B:
         slots = [B.add(s) for s in specs]
         best = B.tune(steps_per_trial=3)
-        assert best["kernel"] in ("flat", "sweep8", "sweep4")
+        assert best["kernel"] in T.SHAPE_NAMES.values()
         assert best["threads"] in (128, 256, 512) and best["cells"] % best["threads"] == 0
         shape = B.shape()
         assert all(shape[k] == best[k] for k in ("kernel", "threads", "cells", "zchunk"))
@@ -124,13 +124,14 @@ def test_wrong_precision_rejected(gpu):
             B.add(_specs(T.TMX_FP32)[0])
 
 
-@pytest.mark.parametrize("tile_y,zchunk", [(8, 3), (4, 1), (8, 64)])
-def test_sweep_shapes_agree(gpu, tile_y, zchunk):
+@pytest.mark.parametrize("kind,zchunk", [(T.SHAPE_SWEEP8, 3), (T.SHAPE_SWEEP4, 1), (T.SHAPE_SWEEP8, 64),
+                                         (T.SHAPE_SWEEP4P, 4), (T.SHAPE_SWEEP2P, 64)])
+def test_sweep_shapes_agree(gpu, kind, zchunk):
     """The FP16 form's sweep interior kernel in a batch (tiles of every mixer
     in one list) gives each mixer its solo run's bits."""
     specs = _specs(T.TMX_FP16)
     with T.Batch(T.TMX_FP16, budget=1 << 28) as B:
-        B.set_sweep(tile_y, zchunk)
+        B.set_sweep(kind, zchunk)
         slots = [B.add(s) for s in specs]
         B.step(6)
         late = B.add(specs[1])
@@ -138,6 +139,6 @@ def test_sweep_shapes_agree(gpu, tile_y, zchunk):
         for slot, spec in zip(slots, specs):
             _same(B, slot, _alone(spec, 11), 11)
         _same(B, late, _alone(specs[1], 5), 5)
-        assert B.shape()["kernel"] == "sweep%d" % tile_y
+        assert B.shape()["kernel"] == T.SHAPE_NAMES[kind]
         B.set_shape(256, 4096)
         assert B.shape()["kernel"] == "flat"

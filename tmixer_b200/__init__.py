@@ -390,8 +390,9 @@ class Solver:
 
     def set_shape(self, kind: int, zchunk: int = 8) -> "Solver":
         """Launch shape of the interior kernel (tmx_set_shape): SHAPE_FLAT, or
-        for the FP16 form SHAPE_SWEEP8 / SHAPE_SWEEP4 with zchunk planes per
-        tile.  Every shape gives the same bits."""
+        for the FP16 form a sweep shape (SHAPE_SWEEP8, SHAPE_SWEEP4, and with
+        the populations prefetched SHAPE_SWEEP4P, SHAPE_SWEEP2P) with zchunk
+        planes per tile.  Every shape gives the same bits."""
         _check(lib().tmx_set_shape(self._h, int(kind), int(zchunk)))
         return self
 
@@ -499,16 +500,15 @@ class Batch:
         """The flat interior kernel with this block size and cell-block size."""
         _check(lib().tmx_batch_set_shape(self._b, int(threads), int(cells)))
 
-    def set_sweep(self, tile_y: int, zchunk: int) -> None:
-        """The FP16 form's sweep interior kernel: tiles of 32 x tile_y nodes
-        walked through zchunk planes."""
-        _check(lib().tmx_batch_set_sweep(self._b, int(tile_y), int(zchunk)))
+    def set_sweep(self, kind: int, zchunk: int) -> None:
+        """One of the FP16 form's sweep interior kernels (a SHAPE_SWEEP* kind)
+        with zchunk planes per tile."""
+        _check(lib().tmx_batch_set_sweep(self._b, int(kind), int(zchunk)))
 
     def shape(self) -> dict:
         o = (ctypes.c_int * 4)()
         _check(lib().tmx_batch_shape(self._b, o))
-        kind = {SHAPE_FLAT: "flat", SHAPE_SWEEP8: "sweep8", SHAPE_SWEEP4: "sweep4"}[o[0]]
-        return dict(kernel=kind, threads=o[1], cells=o[2], zchunk=o[3],
+        return dict(kernel=SHAPE_NAMES[o[0]], threads=o[1], cells=o[2], zchunk=o[3],
                     nodes_per_thread=(o[2] // o[1]) if o[0] == SHAPE_FLAT else o[3])
 
     def set_from(self, shape: dict) -> None:
@@ -516,7 +516,7 @@ class Batch:
         if shape["kernel"] == "flat":
             self.set_shape(shape["threads"], shape["cells"])
         else:
-            self.set_sweep(8 if shape["kernel"] == "sweep8" else 4, shape["zchunk"])
+            self.set_sweep(SHAPE_KINDS[shape["kernel"]], shape["zchunk"])
 
     def tune(self, steps_per_trial: int = 20) -> dict:
         """Autotune the interior kernel's shape (tmx_batch_tune) and return it
@@ -564,7 +564,10 @@ class Request:
                          float(self.tol))
 
 
-SHAPE_FLAT, SHAPE_SWEEP8, SHAPE_SWEEP4 = 0, 1, 2
+SHAPE_FLAT, SHAPE_SWEEP8, SHAPE_SWEEP4, SHAPE_SWEEP4P, SHAPE_SWEEP2P = 0, 1, 2, 3, 4
+SHAPE_NAMES = {SHAPE_FLAT: "flat", SHAPE_SWEEP8: "sweep8", SHAPE_SWEEP4: "sweep4", SHAPE_SWEEP4P: "sweep4p",
+               SHAPE_SWEEP2P: "sweep2p"}
+SHAPE_KINDS = {v: k for k, v in SHAPE_NAMES.items()}
 
 SERVE_STATUS = {0: "converged", 1: "max_steps", -2: "too large for the budget", -5: "non-finite"}
 
@@ -660,5 +663,5 @@ def serve_with(engine, requests, check_every: int = 100, max_active: int = 0):
     return _serve_out(reqs, res[:len(reqs)], summ)
 
 
-__all__ = ["SHAPE_FLAT", "SHAPE_SWEEP8", "SHAPE_SWEEP4", "CaseSpec", "Solver", "Batch", "Request", "serve", "serve_with", "TmxError", "FIELDS", "TMX_FP64", "TMX_FP32", "TMX_FP16", "PRECISIONS",
+__all__ = ["SHAPE_FLAT", "SHAPE_SWEEP8", "SHAPE_SWEEP4", "SHAPE_SWEEP4P", "SHAPE_SWEEP2P", "CaseSpec", "Solver", "Batch", "Request", "serve", "serve_with", "TmxError", "FIELDS", "TMX_FP64", "TMX_FP32", "TMX_FP16", "PRECISIONS",
            "reference_case", "w_layout", "lib"]

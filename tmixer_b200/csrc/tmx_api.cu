@@ -97,15 +97,13 @@ namespace tmx_host {
 
 // The FP16 form's equilibrium polynomial (tmx_engine.cuh poly_q_rn), in host
 // single precision with every operation rounded on its own.
-float poly_q_host(int q, float ux, float uy, float uz)
+float poly_q_host(int q, float ux, float uy, float uz, float omt)
 {
     const int ex = tmx::EX(q), ey = tmx::EY(q), ez = tmx::EZ(q);
-    const float u2 = (ux * ux + uy * uy) + uz * uz;
-    const float t = 1.5f * u2;
-    if (q == 0) return 1.0f - t;
+    if (q == 0) return omt;
     const float a = ex > 0 ? ux : -ux, b = ey > 0 ? uy : -uy, c = ez > 0 ? uz : -uz;
     const float eu = ex ? (ey ? a + b : (ez ? a + c : a)) : (ey ? (ez ? b + c : b) : c);
-    return ((1.0f + 3.0f * eu) - t) + (4.5f * eu) * eu;
+    return std::fmaf(eu, std::fmaf(4.5f, eu, 3.0f), omt);
 }
 
 // IEEE binary16 bits to float (host side of tmx_populations)
@@ -476,10 +474,9 @@ int enqueue_step(tmx_handle* h, int cur, int write_macro, cudaEvent_t* ev)
         TMX_CK(cudaStreamWaitEvent(h->stream, h->join2, 0));
     }
     if (ev) TMX_CK(cudaEventRecord(ev[0], h->stream));
-    if (h->shape == TMX_SHAPE_SWEEP8)
-        tmx::k_sweep8_f16<<<h->sweep_blocks, 256, 0, h->stream>>>(X, G, h->P, write_macro, h->tiles, h->ntiles);
-    else if (h->shape == TMX_SHAPE_SWEEP4)
-        tmx::k_sweep4_f16<<<h->sweep_blocks, 128, 0, h->stream>>>(X, G, h->P, write_macro, h->tiles, h->ntiles);
+    if (const SweepShape* sh = sweep_shape(h->shape))
+        sh->single<<<h->sweep_blocks, sh->threads(), sh->smem(), h->stream>>>(X, G, h->P, write_macro, h->tiles,
+                                                                             h->ntiles);
     else
         h->K->bulk<<<h->bulk_blocks, 256, 0, h->stream>>>(X, G, h->P, write_macro);
     if (ev) TMX_CK(cudaEventRecord(ev[1], h->stream));
@@ -742,17 +739,17 @@ int tmx_create(const tmx_case* c, int device, tmx_handle** out)
 int tmx_set_shape(tmx_handle* h, int kind, int zchunk)
 {
     if (!h) return fail(TMX_E_INVALID, "null handle");
-    if (kind != TMX_SHAPE_FLAT && kind != TMX_SHAPE_SWEEP8 && kind != TMX_SHAPE_SWEEP4)
-        return fail(TMX_E_INVALID, "tmx_set_shape: unknown kind %d", kind);
-    if (kind != TMX_SHAPE_FLAT && !h->K->moments)
+    const SweepShape* sh = sweep_shape(kind);
+    if (kind != TMX_SHAPE_FLAT && !sh) return fail(TMX_E_INVALID, "tmx_set_shape: unknown kind %d", kind);
+    if (sh && !h->K->moments)
         return fail(TMX_E_INVALID, "tmx_set_shape: the sweep shapes are for the FP16 form only");
-    if (kind != TMX_SHAPE_FLAT && zchunk < 1) return fail(TMX_E_INVALID, "tmx_set_shape: zchunk must be >= 1");
+    if (sh && zchunk < 1) return fail(TMX_E_INVALID, "tmx_set_shape: zchunk must be >= 1");
     TMX_CK(cudaSetDevice(h->device));
     TMX_CK(cudaStreamSynchronize(h->stream));
-    if (kind != TMX_SHAPE_FLAT) {
-        const int ty = kind == TMX_SHAPE_SWEEP8 ? 8 : 4;
+    if (sh) {
+        TMX_CK(sweep_allow_smem());
         std::vector<int4> t;
-        sweep_tiles(h->G, 0, ty, zchunk, t);
+        sweep_tiles(h->G, 0, sh->ty, zchunk, t);
         int4* d = nullptr;
         if (!t.empty()) {
             cudaError_t e = cudaMalloc((void**)&d, t.size() * sizeof(int4));
@@ -766,8 +763,7 @@ int tmx_set_shape(tmx_handle* h, int kind, int zchunk)
         }
         int per = 1, sms = 148;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &per, ty == 8 ? (const void*)tmx::k_sweep8_f16 : (const void*)tmx::k_sweep4_f16, 32 * ty, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void*)sh->single, sh->threads(), sh->smem());
         cudaGetLastError();
         cudaFree(h->tiles);
         h->tiles = d;
@@ -968,7 +964,7 @@ int tmx_populations(tmx_handle* h, int box, int fld, double* host_out)
     // the writing node's moments exactly as the kernels do (tmx_engine.cuh)
     std::vector<double> wide(n);
     std::vector<unsigned char> raw(4 * n * h->sbytes);
-    // moment records {(rho, ux, uy, uz), (cA, cB, cC, t)}, 8 floats per node
+    // moment records {(rho, ux, uy, uz), (cA, cB, cC, 1 - 1.5|u|^2)}, 8 floats per node
     std::vector<float> mr(8 * n);
     if (h->K->moments) {
         const float4* m = h->mom[h->cur];
@@ -990,7 +986,8 @@ int tmx_populations(tmx_handle* h, int box, int fld, double* host_out)
                 std::memcpy(&hb, &raw[e], 2);
                 const float* rec = &mr[8 * t];
                 const float r = fld == 0 ? rec[0] : rec[3 + fld];
-                v = half_bits_to_float(hb) + r * (poly_q_host(q, rec[1], rec[2], rec[3]) * w);
+                const float pw = poly_q_host(q, rec[1], rec[2], rec[3], rec[7]) * w;
+                v = std::fmaf(r, pw, half_bits_to_float(hb));
             }
             wide[t] = v;
         }

@@ -215,11 +215,11 @@ struct tmx_batch {
     // launch shape
     int variant = 1;     // index into kBulkThreads
     int cells = 4096;    // nodes per cell block
-    int sweep = 0;       // 0: the flat kernel; 8 or 4: the sweep kernel of that tile height
+    int sweep = 0;       // 0: the flat kernel; else the TMX_SHAPE_SWEEP* shape of the interior
     int zchunk = 8;      // planes per sweep tile
     int sms = 148;
     int grid_bulk[3] = {0, 0, 0};
-    int grid_sweep[2] = {0, 0};  // tile height 8, 4
+    int grid_sweep[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // by TMX_SHAPE_SWEEP* kind
     int grid_faces = 0, grid_edges = 0;
     int nblocks = 0, nfaces = 0, nedges = 0, ntiles = 0, nactive = 0;
     cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
@@ -296,7 +296,7 @@ int rebuild(tmx_batch* b)
         desc[m] = desc_of(b, s);
         for (int g0 = 0; g0 < s.G.nnodes; g0 += b->cells)
             blocks.push_back(make_int4((int)m, g0, std::min(b->cells, s.G.nnodes - g0), 0));
-        if (b->sweep) sweep_tiles(s.G, (int)m, b->sweep, b->zchunk, tiles);
+        if (b->sweep) sweep_tiles(s.G, (int)m, sweep_shape(b->sweep)->ty, b->zchunk, tiles);
         for (size_t t = 0; t < s.nodes.size(); t++) {
             const int2 e = make_int2(s.nodes[t], (int)m * 256 + s.cls[t]);
             if ((int)t < s.nface)
@@ -353,12 +353,9 @@ int enqueue(tmx_batch* b, int parity, int write_macro)
         TMX_CK(cudaStreamWaitEvent(b->stream, b->join, 0));
         TMX_CK(cudaStreamWaitEvent(b->stream, b->join2, 0));
     }
-    if (b->sweep == 8)
-        tmx::k_sweep_batch8_f16<<<b->grid_sweep[0], 256, 0, b->stream>>>(b->d_desc, b->d_tiles, b->d_counts, parity,
-                                                                         write_macro);
-    else if (b->sweep == 4)
-        tmx::k_sweep_batch4_f16<<<b->grid_sweep[1], 128, 0, b->stream>>>(b->d_desc, b->d_tiles, b->d_counts, parity,
-                                                                         write_macro);
+    if (const SweepShape* sh = b->sweep ? sweep_shape(b->sweep) : nullptr)
+        sh->batch<<<b->grid_sweep[b->sweep], sh->threads(), sh->smem(), b->stream>>>(b->d_desc, b->d_tiles,
+                                                                                    b->d_counts, parity, write_macro);
     else
         b->B->bulk[b->variant]<<<b->grid_bulk[b->variant], kBulkThreads[b->variant], 0, b->stream>>>(
             b->d_desc, b->d_blocks, b->d_counts, parity, write_macro);
@@ -402,13 +399,13 @@ void set_grids(tmx_batch* b)
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void*)b->B->bulk[v], kBulkThreads[v], 0);
         b->grid_bulk[v] = b->sms * std::max(1, per);
     }
-    if (b->K->moments) {
-        int p8 = 1, p4 = 1;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p8, (const void*)tmx::k_sweep_batch8_f16, 256, 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p4, (const void*)tmx::k_sweep_batch4_f16, 128, 0);
-        b->grid_sweep[0] = b->sms * std::max(1, p8);
-        b->grid_sweep[1] = b->sms * std::max(1, p4);
-    }
+    if (b->K->moments && sweep_allow_smem() == cudaSuccess)
+        for (int kind = TMX_SHAPE_SWEEP8; kind <= TMX_SHAPE_SWEEP2P; kind++) {
+            const SweepShape* sh = sweep_shape(kind);
+            int per = 1;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void*)sh->batch, sh->threads(), sh->smem());
+            b->grid_sweep[kind] = b->sms * std::max(1, per);
+        }
     int pf = 1, pe = 1;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pf, (const void*)b->B->faces, tmx::kBoundaryThreadsHost, 0);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pe, (const void*)b->B->edges, tmx::kBoundaryThreadsHost, 0);
@@ -830,17 +827,17 @@ int tmx_batch_set_shape(tmx_batch* b, int threads, int cells)
     return TMX_OK;
 }
 
-int tmx_batch_set_sweep(tmx_batch* b, int tile_y, int zchunk)
+int tmx_batch_set_sweep(tmx_batch* b, int kind, int zchunk)
 {
     if (!b) return fail(TMX_E_INVALID, "null batch");
-    if (tile_y != 8 && tile_y != 4) return fail(TMX_E_INVALID, "sweep tile height must be 8 or 4 (got %d)", tile_y);
+    if (!sweep_shape(kind)) return fail(TMX_E_INVALID, "tmx_batch_set_sweep: %d is not a sweep shape", kind);
     if (!b->K->moments) return fail(TMX_E_INVALID, "the sweep kernels are for the FP16 form only");
     if (zchunk < 1) return fail(TMX_E_INVALID, "planes per tile must be >= 1");
     TMX_CK(cudaSetDevice(b->device));
     TMX_CK(cudaStreamSynchronize(b->stream));
-    if (tile_y != b->sweep) drop_graphs(b);
-    if (tile_y != b->sweep || zchunk != b->zchunk) b->dirty = true;
-    b->sweep = tile_y;
+    if (kind != b->sweep) drop_graphs(b);
+    if (kind != b->sweep || zchunk != b->zchunk) b->dirty = true;
+    b->sweep = kind;
     b->zchunk = zchunk;
     return TMX_OK;
 }
@@ -848,8 +845,8 @@ int tmx_batch_set_sweep(tmx_batch* b, int tile_y, int zchunk)
 int tmx_batch_shape(const tmx_batch* b, int out[4])
 {
     if (!b || !out) return fail(TMX_E_INVALID, "null argument");
-    out[0] = b->sweep == 8 ? TMX_SHAPE_SWEEP8 : (b->sweep == 4 ? TMX_SHAPE_SWEEP4 : TMX_SHAPE_FLAT);
-    out[1] = b->sweep ? 32 * b->sweep : kBulkThreads[b->variant];
+    out[0] = b->sweep ? b->sweep : TMX_SHAPE_FLAT;
+    out[1] = b->sweep ? sweep_shape(b->sweep)->threads() : kBulkThreads[b->variant];
     out[2] = b->cells;
     out[3] = b->zchunk;
     return TMX_OK;
@@ -898,15 +895,15 @@ int tmx_batch_tune(tmx_batch* b, int steps_per_trial, int* threads_out, int* cel
             }
         }
     if (b->K->moments)
-        for (int ty : {8, 4})
+        for (int kind = TMX_SHAPE_SWEEP8; kind <= TMX_SHAPE_SWEEP2P; kind++)
             for (int zi = 0; zi < 4 && rc == TMX_OK; zi++) {
-                rc = tmx_batch_set_sweep(b, ty, kZChunkChoices[zi]);
+                rc = tmx_batch_set_sweep(b, kind, kZChunkChoices[zi]);
                 if (rc) break;
                 double ms = 0;
                 trial(ms);
                 if (rc == TMX_OK && ms < best) {
                     best = ms;
-                    bs = ty;
+                    bs = kind;
                     bz = kZChunkChoices[zi];
                 }
             }
@@ -925,8 +922,8 @@ int tmx_batch_tune(tmx_batch* b, int steps_per_trial, int* threads_out, int* cel
         }
     b->dirty = true;
     TMX_CK(cudaStreamSynchronize(b->stream));
-    if (threads_out) *threads_out = bs ? 32 * bs : kBulkThreads[bv];
-    if (cells_out) *cells_out = bs ? 32 * bs * bz : bc;
+    if (threads_out) *threads_out = bs ? sweep_shape(bs)->threads() : kBulkThreads[bv];
+    if (cells_out) *cells_out = bs ? sweep_shape(bs)->threads() * bz : bc;
     if (ms_out) *ms_out = best;
     return TMX_OK;
 }

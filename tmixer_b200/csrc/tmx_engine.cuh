@@ -40,29 +40,29 @@ namespace tmx {
 // precision policies
 // ---------------------------------------------------------------------------
 
-// Deterministic FP32 equilibrium polynomial (every operation rounded on its
-// own, no contraction): the FP16 form adds and subtracts this value when it
-// encodes and decodes populations, so both sides must produce the same bits.
-// t = 1.5 |u|^2 is shared by the 19 directions; the FP16 form stores it
-// with the writer's moments so that readers need not recompute it.
-__device__ __forceinline__ float u2_term(float ux, float uy, float uz)
+// FP32 equilibrium polynomial of the reduced-precision forms, evaluated the
+// same way by every caller: P_q = omt + e.u (3 + 4.5 e.u) as two correctly
+// rounded fused multiply-adds, with omt = 1 - 1.5 |u|^2 shared by the 19
+// directions.  The FP16 form adds and subtracts w_q * rho * P_q when it
+// encodes and decodes populations, so writer and reader must produce the same
+// bits from the same inputs: explicit __fmaf_rn / __fmul_rn / __fadd_rn, never
+// left to contraction.  The FP16 form stores omt with the writer's moments so
+// that readers need not recompute it.
+__device__ __forceinline__ float omt_term(float ux, float uy, float uz)
 {
-    return __fmul_rn(1.5f, __fadd_rn(__fadd_rn(__fmul_rn(ux, ux), __fmul_rn(uy, uy)), __fmul_rn(uz, uz)));
+    const float u2 = __fadd_rn(__fadd_rn(__fmul_rn(ux, ux), __fmul_rn(uy, uy)), __fmul_rn(uz, uz));
+    return __fsub_rn(1.0f, __fmul_rn(1.5f, u2));
 }
 // direction given by its lattice vector (ex, ey, ez), possibly run-time values
-__device__ __forceinline__ float poly_e_rn_t(int ex, int ey, int ez, float ux, float uy, float uz, float t)
+__device__ __forceinline__ float poly_e_omt(int ex, int ey, int ez, float ux, float uy, float uz, float omt)
 {
-    if ((ex | ey | ez) == 0) return __fsub_rn(1.0f, t);
+    if ((ex | ey | ez) == 0) return omt;
     const float eu = e_dot_u_e(ex, ey, ez, ux, uy, uz);
-    return __fadd_rn(__fsub_rn(__fadd_rn(1.0f, __fmul_rn(3.0f, eu)), t), __fmul_rn(__fmul_rn(4.5f, eu), eu));
+    return __fmaf_rn(eu, __fmaf_rn(4.5f, eu, 3.0f), omt);
 }
-__device__ __forceinline__ float poly_q_rn_t(int q, float ux, float uy, float uz, float t)
+__device__ __forceinline__ float poly_q_omt(int q, float ux, float uy, float uz, float omt)
 {
-    return poly_e_rn_t(EX(q), EY(q), EZ(q), ux, uy, uz, t);
-}
-__device__ __forceinline__ float poly_q_rn(int q, float ux, float uy, float uz)
-{
-    return poly_q_rn_t(q, ux, uy, uz, u2_term(ux, uy, uz));
+    return poly_e_omt(EX(q), EY(q), EZ(q), ux, uy, uz, omt);
 }
 
 // Collision of one direction of the interleaved forms with sm_100's packed
@@ -181,20 +181,16 @@ struct F32 {
     // poly holds w_q * poly_q, so that an equilibrium value is one multiply
     __device__ static void poly(T ux, T uy, T uz, T (&p)[19])
     {
-        eq_poly(ux, uy, uz, p);
+        const float omt = omt_term(ux, uy, uz);
 #pragma unroll
-        for (int q = 0; q < 19; q++) p[q] = p[q] * (float)wq(q);
+        for (int q = 0; q < 19; q++) p[q] = __fmul_rn(poly_q_omt(q, ux, uy, uz, omt), (float)wq(q));
     }
     __device__ static bool tiny(T) { return false; }
     __device__ static T feq(T r, T pw, int, bool) { return r * pw; }
     // w * poly of one direction given by (ex, ey, ez) and weight w
     __device__ static T pw_dir(int ex, int ey, int ez, T w, T ux, T uy, T uz)
     {
-        const T u2 = ux * ux + uy * uy + uz * uz;
-        const T t = T(3) * u2 / T(2);
-        if ((ex | ey | ez) == 0) return (T(1) - t) * w;
-        const T eu = e_dot_u_e(ex, ey, ez, ux, uy, uz);
-        return (T(1) + T(3) * eu - t + T(9) * eu * eu / T(2)) * w;
+        return __fmul_rn(poly_e_omt(ex, ey, ez, ux, uy, uz, omt_term(ux, uy, uz)), w);
     }
     // the four fields pulled from source s along (ex, ey, ez) of direction q,
     // as the pairs (flow, A), (B, C)
@@ -205,12 +201,22 @@ struct F32 {
         v01 = make_float2(x.x, x.y);
         v23 = make_float2(x.z, x.w);
     }
-    __device__ static void decode_pairs_rec(const S* __restrict__ Pin, long long ps, int q, int, int, int, T, int s,
-                                            const float4&, const float4&, float2& v01, float2& v23)
+    // the stored bytes of (q, s): one 16-byte access
+    using Raw = float4;
+    __device__ static Raw load_raw(const S* __restrict__ Pin, long long ps, int q, int s)
     {
-        const float4 x = __ldg((const float4*)(Pin + off(0, q, ps, s)));
+        return __ldg((const float4*)(Pin + off(0, q, ps, s)));
+    }
+    __device__ static void decode_raw(const Raw& x, int, int, int, T, const float4&, const float4&, float2& v01,
+                                      float2& v23)
+    {
         v01 = make_float2(x.x, x.y);
         v23 = make_float2(x.z, x.w);
+    }
+    __device__ static void decode_pairs_rec(const S* __restrict__ Pin, long long ps, int q, int ex, int ey, int ez,
+                                            T w, int s, const float4& mf, const float4& ms, float2& v01, float2& v23)
+    {
+        decode_raw(load_raw(Pin, ps, q, s), ex, ey, ez, w, mf, ms, v01, v23);
     }
     __device__ static void decode4(const S* __restrict__ Pin, const float4* __restrict__, long long ps, int q, int,
                                    int, int, T, int s, T (&v)[4])
@@ -247,7 +253,7 @@ struct F32 {
 
 // FP32 arithmetic; populations stored in FP16 as their non-equilibrium part
 // n_q = f_q - feq_q(rho, u) of the node that wrote them, next to that node's
-// FP32 moments M = {(rho, ux, uy, uz), (cA, cB, cC, 1.5|u|^2)}, one 32-byte
+// FP32 moments M = {(rho, ux, uy, uz), (cA, cB, cC, 1 - 1.5|u|^2)}, one 32-byte
 // record per node (float4 M[2g], M[2g+1]).  A
 // reader adds back feq_q of the writer's moments.  The stored quantity is of
 // the order of the gradients, so FP16 keeps about FP32 accuracy of f.
@@ -288,18 +294,20 @@ struct F16 {
     __device__ static void poly(T ux, T uy, T uz, T (&p)[19])
     {
 #pragma unroll
-        for (int q = 0; q < 19; q++) p[q] = __fmul_rn(poly_q_rn(q, ux, uy, uz), (float)wq(q));
+        const float omt = omt_term(ux, uy, uz);
+#pragma unroll
+        for (int q = 0; q < 19; q++) p[q] = __fmul_rn(poly_q_omt(q, ux, uy, uz, omt), (float)wq(q));
     }
     __device__ static bool tiny(T) { return false; }
     __device__ static T feq(T r, T pw, int, bool) { return __fmul_rn(r, pw); }
-    // w_q * poly_q of a writer from its moment record {(rho, u), (c, t)}
+    // w_q * poly_q of a writer from its moment record {(rho, u), (c, omt)}
     __device__ static T src_pw(int q, const float4& mf, const float4& ms)
     {
-        return __fmul_rn(poly_q_rn_t(q, mf.y, mf.z, mf.w, ms.w), (float)wq(q));
+        return __fmul_rn(poly_q_omt(q, mf.y, mf.z, mf.w, ms.w), (float)wq(q));
     }
     __device__ static T pw_dir(int ex, int ey, int ez, T w, T ux, T uy, T uz)
     {
-        return __fmul_rn(poly_e_rn_t(ex, ey, ez, ux, uy, uz, u2_term(ux, uy, uz)), w);
+        return __fmul_rn(poly_e_omt(ex, ey, ez, ux, uy, uz, omt_term(ux, uy, uz)), w);
     }
     // the four fields pulled from source s along (ex, ey, ez) of direction q,
     // as the pairs (flow, A), (B, C): the stored part plus the writer's
@@ -310,16 +318,27 @@ struct F16 {
         const float4 mf = __ldg(M + 2 * (long long)s), ms = __ldg(M + 2 * (long long)s + 1);
         decode_pairs_rec(Pin, ps, q, ex, ey, ez, w, s, mf, ms, v01, v23);
     }
+    // the stored bytes of (q, s): one 8-byte access
+    using Raw = uint2;
+    __device__ static Raw load_raw(const S* __restrict__ Pin, long long ps, int q, int s)
+    {
+        return __ldg((const uint2*)(Pin + off(0, q, ps, s)));
+    }
     // the same with the writer's record {mf, ms} given
     __device__ static void decode_pairs_rec(const S* __restrict__ Pin, long long ps, int q, int ex, int ey, int ez,
                                             T w, int s, const float4& mf, const float4& ms, float2& v01, float2& v23)
     {
-        const uint2 x = __ldg((const uint2*)(Pin + off(0, q, ps, s)));
+        decode_raw(load_raw(Pin, ps, q, s), ex, ey, ez, w, mf, ms, v01, v23);
+    }
+    // ... and with the stored bytes given
+    __device__ static void decode_raw(const Raw& x, int ex, int ey, int ez, T w, const float4& mf, const float4& ms,
+                                      float2& v01, float2& v23)
+    {
         const float2 raw01 = __half22float2(*(const __half2*)&x.x), raw23 = __half22float2(*(const __half2*)&x.y);
-        const float pw = __fmul_rn(poly_e_rn_t(ex, ey, ez, mf.y, mf.z, mf.w, ms.w), w);
+        const float pw = __fmul_rn(poly_e_omt(ex, ey, ez, mf.y, mf.z, mf.w, ms.w), w);
         const float2 pp = make_float2(pw, pw);
-        v01 = __fadd2_rn(raw01, __fmul2_rn(make_float2(mf.x, ms.x), pp));
-        v23 = __fadd2_rn(raw23, __fmul2_rn(make_float2(ms.y, ms.z), pp));
+        v01 = __ffma2_rn(make_float2(mf.x, ms.x), pp, raw01);
+        v23 = __ffma2_rn(make_float2(ms.y, ms.z), pp, raw23);
     }
     __device__ static void decode4(const S* __restrict__ Pin, const float4* __restrict__ M, long long ps, int q,
                                    int ex, int ey, int ez, T w, int s, T (&v)[4])
@@ -548,7 +567,7 @@ __device__ __forceinline__ void bulk_node(const StepPtrs& X, const Geom& G, cons
     if (PR::kMoments) {
         X.mcur[2 * (long long)g] = make_float4((float)rho, (float)ux, (float)uy, (float)uz);
         X.mcur[2 * (long long)g + 1] =
-            make_float4((float)ca, (float)cb, (float)cc, u2_term((float)ux, (float)uy, (float)uz));
+            make_float4((float)ca, (float)cb, (float)cc, omt_term((float)ux, (float)uy, (float)uz));
     }
     if (write_macro) {
         double* Mac = X.mac;
@@ -588,14 +607,32 @@ struct RecShared {
     }
 };
 
+// The stored populations of a source for lp_interior: loaded from global
+// memory (the flat bulk kernel and the sweep kernels without prefetch) ...
+template <class PR>
+struct PopGlobal {
+    const typename PR::S* __restrict__ Pin;
+    long long ps;
+    __device__ __forceinline__ typename PR::Raw operator()(int q, int s) const { return PR::load_raw(Pin, ps, q, s); }
+};
+// ... or from the copy a sweep kernel prefetched into shared memory for this
+// thread: direction q at base[q * stride].
+template <class PR>
+struct PopStaged {
+    const typename PR::Raw* base;
+    int stride;
+    __device__ __forceinline__ typename PR::Raw operator()(int q, int) const { return base[q * stride]; }
+};
+
 // One interior node (b, i, j, k) = g for the reduced-precision forms (FP32
 // arithmetic): every source index and (FP16 form) every writer's record
 // (from rec) is fetched once per direction and all 76 populations decoded in
 // one pass, which the FP32 register budget affords (the FP64 form loads field
-// by field).  The arithmetic does not depend on where the records come from.
-template <class PR, class Rec>
+// by field).  The arithmetic does not depend on where the records and the
+// stored populations (pop) come from.
+template <class PR, class Rec, class Pop>
 __device__ __forceinline__ void lp_interior(const StepPtrs& X, const Geom& G, const Phys& P, int write_macro, int g,
-                                            int b, int i, int j, int k, const Rec& rec)
+                                            int b, int i, int j, int k, const Rec& rec, const Pop& pop)
 {
     using T = typename PR::T;
     const typename PR::S* __restrict__ Pin = (const typename PR::S*)X.pin;
@@ -611,7 +648,7 @@ __device__ __forceinline__ void lp_interior(const StepPtrs& X, const Geom& G, co
         const int s = bulk_src(G, g, i, k, sy, sz, iface, q);
         float4 mf = make_float4(0.f, 0.f, 0.f, 0.f), ms = mf;
         if constexpr (PR::kMoments) rec(q, s, mf, ms);
-        PR::decode_pairs_rec(Pin, ps, q, EX(q), EY(q), EZ(q), (float)wq(q), s, mf, ms, p01[q], p23[q]);
+        PR::decode_raw(pop(q, s), EX(q), EY(q), EZ(q), (float)wq(q), mf, ms, p01[q], p23[q]);
     }
     // sums in index order, two fields at a time
     float2 s01 = p01[0], s23 = p23[0];
@@ -649,7 +686,7 @@ __device__ __forceinline__ void lp_interior(const StepPtrs& X, const Geom& G, co
     if (PR::kMoments) {
         X.mcur[2 * (long long)g] = make_float4((float)rho, (float)ux, (float)uy, (float)uz);
         X.mcur[2 * (long long)g + 1] =
-            make_float4((float)ca, (float)cb, (float)cc, u2_term((float)ux, (float)uy, (float)uz));
+            make_float4((float)ca, (float)cb, (float)cc, omt_term((float)ux, (float)uy, (float)uz));
     }
     if (write_macro) {
         double* Mac = X.mac;
@@ -670,7 +707,8 @@ __device__ __forceinline__ void bulk_node_lp(const StepPtrs& X, const Geom& G, c
     int b, i, j, k;
     decode(G, g, b, i, j, k);
     if (is_boundary(G, b, i, j, k)) return;
-    lp_interior<PR>(X, G, P, write_macro, g, b, i, j, k, RecGlobal{X.mprev});
+    lp_interior<PR>(X, G, P, write_macro, g, b, i, j, k, RecGlobal{X.mprev},
+                    PopGlobal<PR>{(const typename PR::S*)X.pin, G.ps});
 }
 
 // ---------------------------------------------------------------------------
@@ -715,24 +753,38 @@ __device__ __forceinline__ int tile_rec_node(const Geom& G, int b, int x, int y,
     return -1;
 }
 
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem)
+{
+    const unsigned a = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(a), "l"(gmem) : "memory");
+}
+
 // One tile {mixer * 2 + box, x0 | y0 << 16, z0 | z1 << 16} (0-based x0, y0;
 // interior planes z0 .. z1-1, 2 <= z0 < z1 <= nz).  A and B hold the two
-// halves of 4 * (TY + 2) * 34 records.  Every thread of the block runs the
-// same iterations (the barriers are uniform).
-template <class PR, int TY>
+// halves of 4 * (TY + 2) * 34 records.  With PF the populations are
+// pipelined too: each thread copies the 19 stored values its node of plane
+// k + 1 will read into its slots of PS (two planes of 19 x 32 TY values,
+// 8 bytes each) while it computes plane k, so the loads of both kinds are in
+// flight during the arithmetic.  Every thread of the block runs the same
+// iterations (the barriers are uniform).
+template <class PR, int TY, bool PF>
 __device__ __forceinline__ void sweep_tile(const StepPtrs& X, const Geom& G, const Phys& P, int write_macro, int4 t,
-                                           float4* A, float4* B)
+                                           float4* A, float4* B, typename PR::Raw* PS)
 {
-    constexpr int RW = kSweepX + 2, PLANE = (TY + 2) * RW;
+    constexpr int RW = kSweepX + 2, PLANE = (TY + 2) * RW, NT = kSweepX * TY;
     const int b = t.x & 1;
     const int x0 = t.y & 0xffff, y0 = t.y >> 16, z0 = t.z & 0xffff, z1 = t.z >> 16;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     const int nx = box_nx(G, b), ny = box_ny(G, b);
     const int x = x0 + tx, y = y0 + ty;
+    const bool in_box = x < nx && y < ny;
+    const int sy = nx, sz = nx * ny;
+    const int iface = (b == 0 && y == 0) ? 1 : ((b == 1 && y == G.mny - 1) ? 2 : 0);
     const float4* __restrict__ M = X.mprev;
+    const typename PR::S* __restrict__ Pin = (const typename PR::S*)X.pin;
     auto stage = [&](int kk) {
         const int slot = (kk & 3) * PLANE;
-        for (int e = threadIdx.x; e < PLANE; e += kSweepX * TY) {
+        for (int e = threadIdx.x; e < PLANE; e += NT) {
             const int ry = e / RW, rx = e - ry * RW;
             const int n = tile_rec_node(G, b, x0 + rx - 1, y0 + ry - 1, kk);
             if (n >= 0) {
@@ -741,20 +793,42 @@ __device__ __forceinline__ void sweep_tile(const StepPtrs& X, const Geom& G, con
             }
         }
     };
+    // this thread's 19 stored values of plane kk (interior nodes only)
+    auto prefetch = [&](int kk) {
+        if (!in_box || is_boundary(G, b, x + 1, y + 1, kk)) return;
+        const int g = box_base(G, b) + ((kk - 1) * ny + y) * nx + x;
+        typename PR::Raw* dst = PS + (kk & 1) * 19 * NT + threadIdx.x;
+#pragma unroll
+        for (int q = 0; q < 19; q++) {
+            const int s = bulk_src(G, g, x + 1, kk, sy, sz, iface, q);
+            cp_async8(dst + q * NT, Pin + PR::off(0, q, G.ps, s));
+        }
+    };
     stage(z0 - 1);
     stage(z0);
     stage(z0 + 1);
+    if constexpr (PF) prefetch(z0);
     cp_async_commit();
     cp_async_wait_all();
     __syncthreads();
     for (int k = z0; k < z1; k++) {
         // plane k + 2 goes to the slot of plane k - 2, which no thread reads
-        // any more (the barrier at the end of the previous iteration)
+        // any more (the barrier at the end of the previous iteration); the
+        // populations of plane k + 1 to the other half of PS, which this
+        // thread finished reading in the previous iteration
         if (k + 2 < z1 + 1) stage(k + 2);
+        if constexpr (PF)
+            if (k + 1 < z1) prefetch(k + 1);
         cp_async_commit();
-        if (x < nx && y < ny && !is_boundary(G, b, x + 1, y + 1, k))
-            lp_interior<PR>(X, G, P, write_macro, box_base(G, b) + ((k - 1) * ny + y) * nx + x, b, x + 1, y + 1, k,
-                            RecShared<TY>{A, B, tx, ty, k});
+        if (in_box && !is_boundary(G, b, x + 1, y + 1, k)) {
+            const int g = box_base(G, b) + ((k - 1) * ny + y) * nx + x;
+            if constexpr (PF)
+                lp_interior<PR>(X, G, P, write_macro, g, b, x + 1, y + 1, k, RecShared<TY>{A, B, tx, ty, k},
+                                PopStaged<PR>{PS + (k & 1) * 19 * NT + threadIdx.x, NT});
+            else
+                lp_interior<PR>(X, G, P, write_macro, g, b, x + 1, y + 1, k, RecShared<TY>{A, B, tx, ty, k},
+                                PopGlobal<PR>{Pin, G.ps});
+        }
         cp_async_wait_all();
         __syncthreads();
     }
@@ -1359,7 +1433,7 @@ __device__ __forceinline__ void boundary_lane(const StepPtrs& X, const Geom& G, 
         if (fld == 0) X.mcur[2 * (long long)c.g] = make_float4((float)rho, (float)ux, (float)uy, (float)uz);
         if (fld == 1)
             X.mcur[2 * (long long)c.g + 1] =
-                make_float4((float)ca, (float)cb, (float)cc, u2_term((float)ux, (float)uy, (float)uz));
+                make_float4((float)ca, (float)cb, (float)cc, omt_term((float)ux, (float)uy, (float)uz));
     }
     if (write_macro) {
         Mac[(fld == 0 ? 0 : 3 + fld) * ps + c.g] = r;
@@ -1515,7 +1589,7 @@ __device__ __forceinline__ void boundary_lane_lp(const StepPtrs& X, const Geom& 
         if (fld == 0) X.mcur[2 * (long long)c.g] = make_float4((float)rho, (float)ux, (float)uy, (float)uz);
         if (fld == 1)
             X.mcur[2 * (long long)c.g + 1] =
-                make_float4((float)ca, (float)cb, (float)cc, u2_term((float)ux, (float)uy, (float)uz));
+                make_float4((float)ca, (float)cb, (float)cc, omt_term((float)ux, (float)uy, (float)uz));
     }
     if (write_macro) {
         Mac[(fld == 0 ? 0 : 3 + fld) * ps + c.g] = r;
@@ -1581,43 +1655,45 @@ __device__ __forceinline__ void bulk_any(const StepPtrs& X, const Geom& G, const
             bulk_any<PR>(X, G, P, write_macro, g);                                                              \
     }
 
-// The FP16 form's interior as tiles (sweep_tile): 32 x 8 threads (two blocks
-// per SM) or 32 x 4 (four), persistent over the tile list.
-#define TMX_DEFINE_SWEEP_KERNELS(PR, NAME)                                                                        \
-    __global__ void __launch_bounds__(256, 2) k_sweep8_##NAME(StepPtrs X, Geom G, Phys P, int write_macro,      \
-                                                              const int4* __restrict__ tiles, int ntiles)       \
+// The FP16 form's interior as tiles (sweep_tile), persistent over the tile
+// list: 32 x 8 threads (two blocks per SM) or 32 x 4 (four), and with the
+// populations pipelined 32 x 4 (three) or 32 x 2 (six).  The pipelined
+// 32 x 4 kernel takes its 65,024 bytes of shared memory dynamically.
+constexpr int sweep_smem_bytes(int ty, bool pf)
+{
+    return 2 * 4 * (ty + 2) * (kSweepX + 2) * 16 + (pf ? 2 * 19 * kSweepX * ty * 8 : 0);
+}
+#define TMX_SWEEP_KERNEL(PR, NAME, TY, PF, SUFFIX, MINB)                                                          \
+    __global__ void __launch_bounds__(kSweepX * TY, MINB) k_sweep##SUFFIX##_##NAME(                              \
+        StepPtrs X, Geom G, Phys P, int write_macro, const int4* __restrict__ tiles, int ntiles)                 \
     {                                                                                                           \
-        __shared__ float4 A[4 * 10 * (kSweepX + 2)], B[4 * 10 * (kSweepX + 2)];                                 \
-        for (int t = blockIdx.x; t < ntiles; t += gridDim.x) sweep_tile<PR, 8>(X, G, P, write_macro, tiles[t], A, B); \
+        extern __shared__ float4 sweep_smem[];                                                                  \
+        float4* A = sweep_smem;                                                                                 \
+        float4* B = A + 4 * (TY + 2) * (kSweepX + 2);                                                           \
+        PR::Raw* PS = (PR::Raw*)(B + 4 * (TY + 2) * (kSweepX + 2));                                             \
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x)                                                    \
+            sweep_tile<PR, TY, PF>(X, G, P, write_macro, tiles[t], A, B, PS);                                   \
     }                                                                                                           \
-    __global__ void __launch_bounds__(128, 4) k_sweep4_##NAME(StepPtrs X, Geom G, Phys P, int write_macro,      \
-                                                              const int4* __restrict__ tiles, int ntiles)       \
+    __global__ void __launch_bounds__(kSweepX * TY, MINB) k_sweep_batch##SUFFIX##_##NAME(                        \
+        const MixerDesc* __restrict__ D, const int4* __restrict__ tiles, const int* __restrict__ counts,         \
+        int parity, int write_macro)                                                                            \
     {                                                                                                           \
-        __shared__ float4 A[4 * 6 * (kSweepX + 2)], B[4 * 6 * (kSweepX + 2)];                                   \
-        for (int t = blockIdx.x; t < ntiles; t += gridDim.x) sweep_tile<PR, 4>(X, G, P, write_macro, tiles[t], A, B); \
-    }                                                                                                           \
-    __global__ void __launch_bounds__(256, 2) k_sweep_batch8_##NAME(const MixerDesc* __restrict__ D,            \
-        const int4* __restrict__ tiles, const int* __restrict__ counts, int parity, int write_macro)            \
-    {                                                                                                           \
-        __shared__ float4 A[4 * 10 * (kSweepX + 2)], B[4 * 10 * (kSweepX + 2)];                                 \
+        extern __shared__ float4 sweep_smem[];                                                                  \
+        float4* A = sweep_smem;                                                                                 \
+        float4* B = A + 4 * (TY + 2) * (kSweepX + 2);                                                           \
+        PR::Raw* PS = (PR::Raw*)(B + 4 * (TY + 2) * (kSweepX + 2));                                             \
         const int n = counts[3];                                                                                \
         for (int t = blockIdx.x; t < n; t += gridDim.x) {                                                       \
             const int4 tl = tiles[t];                                                                           \
             const MixerDesc& d = D[tl.x >> 1];                                                                  \
-            sweep_tile<PR, 8>(d.X[parity], d.G, d.P, write_macro, tl, A, B);                                    \
-        }                                                                                                       \
-    }                                                                                                           \
-    __global__ void __launch_bounds__(128, 4) k_sweep_batch4_##NAME(const MixerDesc* __restrict__ D,            \
-        const int4* __restrict__ tiles, const int* __restrict__ counts, int parity, int write_macro)            \
-    {                                                                                                           \
-        __shared__ float4 A[4 * 6 * (kSweepX + 2)], B[4 * 6 * (kSweepX + 2)];                                   \
-        const int n = counts[3];                                                                                \
-        for (int t = blockIdx.x; t < n; t += gridDim.x) {                                                       \
-            const int4 tl = tiles[t];                                                                           \
-            const MixerDesc& d = D[tl.x >> 1];                                                                  \
-            sweep_tile<PR, 4>(d.X[parity], d.G, d.P, write_macro, tl, A, B);                                    \
+            sweep_tile<PR, TY, PF>(d.X[parity], d.G, d.P, write_macro, tl, A, B, PS);                           \
         }                                                                                                       \
     }
+#define TMX_DEFINE_SWEEP_KERNELS(PR, NAME)        \
+    TMX_SWEEP_KERNEL(PR, NAME, 8, false, 8, 2)    \
+    TMX_SWEEP_KERNEL(PR, NAME, 4, false, 4, 4)    \
+    TMX_SWEEP_KERNEL(PR, NAME, 4, true, 4p, 3)    \
+    TMX_SWEEP_KERNEL(PR, NAME, 2, true, 2p, 6)
 
 // The face and the edge list as two launches (the FP32 and FP16-storage steps;
 // the FP64 step uses k_bound and k_walls).
