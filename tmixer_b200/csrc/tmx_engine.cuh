@@ -471,7 +471,7 @@ __device__ __forceinline__ void init_node(const StepPtrs& X, const Geom& G, cons
     for (int m = 1; m < 7; m++) Mac[m * ps + g] = 0.0;
     if (PR::kMoments) {
         X.mcur[2 * (long long)g] = make_float4((float)rho0, 0.f, 0.f, 0.f);
-        X.mcur[2 * (long long)g + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
+        X.mcur[2 * (long long)g + 1] = make_float4(0.f, 0.f, 0.f, omt_term(0.f, 0.f, 0.f));
     }
 }
 
