@@ -400,7 +400,7 @@ void set_grids(tmx_batch* b)
         b->grid_bulk[v] = b->sms * std::max(1, per);
     }
     if (b->K->moments && sweep_allow_smem() == cudaSuccess)
-        for (int kind = TMX_SHAPE_SWEEP8; kind <= TMX_SHAPE_SWEEP8L; kind++) {
+        for (int kind = TMX_SHAPE_SWEEP8; kind <= TMX_SHAPE_SWEEP2P; kind++) {
             const SweepShape* sh = sweep_shape(kind);
             int per = 1;
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void*)sh->batch, sh->threads(), sh->smem());
@@ -895,7 +895,7 @@ int tmx_batch_tune(tmx_batch* b, int steps_per_trial, int* threads_out, int* cel
             }
         }
     if (b->K->moments)
-        for (int kind = TMX_SHAPE_SWEEP8; kind <= TMX_SHAPE_SWEEP8L; kind++)
+        for (int kind = TMX_SHAPE_SWEEP8; kind <= TMX_SHAPE_SWEEP2P; kind++)
             for (int zi = 0; zi < 4 && rc == TMX_OK; zi++) {
                 rc = tmx_batch_set_sweep(b, kind, kZChunkChoices[zi]);
                 if (rc) break;

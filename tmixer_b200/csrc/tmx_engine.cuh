@@ -607,14 +607,23 @@ struct RecShared {
     }
 };
 
-// The stored populations of a source for lp_interior, loaded from global
-// memory.
+// The stored populations of a source for lp_interior: loaded from global
+// memory (the flat bulk kernel and the sweep kernels without prefetch) ...
 template <class PR>
 struct PopGlobal {
     const typename PR::S* __restrict__ Pin;
     long long ps;
     __device__ __forceinline__ typename PR::Raw operator()(int q, int s) const { return PR::load_raw(Pin, ps, q, s); }
 };
+// ... or from the copy a sweep kernel prefetched into shared memory for this
+// thread: direction q at base[q * stride].
+template <class PR>
+struct PopStaged {
+    const typename PR::Raw* base;
+    int stride;
+    __device__ __forceinline__ typename PR::Raw operator()(int q, int) const { return base[q * stride]; }
+};
+
 // One interior node (b, i, j, k) = g for the reduced-precision forms (FP32
 // arithmetic): every source index and (FP16 form) every writer's record
 // (from rec) is fetched once per direction and all 76 populations decoded in
@@ -744,99 +753,23 @@ __device__ __forceinline__ int tile_rec_node(const Geom& G, int b, int x, int y,
     return -1;
 }
 
-// lp_interior in two passes over the node's 19 sources, holding only their
-// stored bytes (38 registers for the FP16 form instead of 76 decoded values):
-// pass 1 decodes each direction and accumulates the densities and the
-// momentum, pass 2 decodes it again (the writer's record is re-read from the
-// sweep tile's shared memory) and collides.  The sums and the momentum
-// accumulate term by term in index order, the operations of sum19 and
-// momentum, so the results are lp_interior's bit for bit; the lower register
-// count lets a sweep block keep about twice as many nodes in flight.
-template <class PR, int TY>
-__device__ __forceinline__ void lp_interior_2p(const StepPtrs& X, const Geom& G, const Phys& P, int write_macro,
-                                               int g, int b, int i, int j, int k, const RecShared<TY>& rec)
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem)
 {
-    using T = typename PR::T;
-    const typename PR::S* __restrict__ Pin = (const typename PR::S*)X.pin;
-    typename PR::S* __restrict__ Pout = (typename PR::S*)X.pout;
-    const long long ps = G.ps;
-    const int sy = box_nx(G, b), sz = box_nx(G, b) * box_ny(G, b);
-    const int iface = (b == 0 && j == 1) ? 1 : ((b == 1 && j == G.mny) ? 2 : 0);
-    typename PR::Raw raw[19];
-#pragma unroll
-    for (int q = 0; q < 19; q++) raw[q] = PR::load_raw(Pin, ps, q, bulk_src(G, g, i, k, sy, sz, iface, q));
-    // pass 1: densities (index order, two fields at a time) and momentum
-    // (each component's terms in index order, as momentum() writes them)
-    float2 s01 = make_float2(0.f, 0.f), s23 = s01;
-    T mx = T(0), my = T(0), mz = T(0);
-#pragma unroll
-    for (int q = 0; q < 19; q++) {
-        float4 mf, ms;
-        rec(q, 0, mf, ms);
-        float2 v01, v23;
-        PR::decode_raw(raw[q], EX(q), EY(q), EZ(q), (float)wq(q), mf, ms, v01, v23);
-        if (q == 0) {
-            s01 = v01;
-            s23 = v23;
-        } else {
-            s01 = __fadd2_rn(s01, v01);
-            s23 = __fadd2_rn(s23, v23);
-        }
-        const T f = v01.x;
-        if (EX(q) != 0) mx = (q == 1) ? f : (EX(q) > 0 ? mx + f : mx - f);
-        if (EY(q) != 0) my = (q == 2) ? f : (EY(q) > 0 ? my + f : my - f);
-        if (EZ(q) != 0) mz = (q == 5) ? f : (EZ(q) > 0 ? mz + f : mz - f);
-    }
-    const T rho = s01.x, ca = s01.y, cb = s23.x, cc = s23.y;
-    const T ux = mx / rho, uy = my / rho, uz = mz / rho;
-    const float omt = omt_term(ux, uy, uz);
-    const T rt = T(P.rateconst) * ca * cb;
-    const float2 r01 = make_float2(rho, ca), r23 = make_float2(cb, cc);
-    const float2 c1a = make_float2((float)P.c1[0], (float)P.c1[1]), c1b = make_float2((float)P.c1[2], (float)P.c1[3]);
-    const float2 c2a = make_float2((float)P.c2[0], (float)P.c2[1]), c2b = make_float2((float)P.c2[2], (float)P.c2[3]);
-    // pass 2: decode again, collide, store
-#pragma unroll
-    for (int q = 0; q < 19; q++) {
-        float4 mf, ms;
-        rec(q, 0, mf, ms);
-        float2 v01, v23;
-        PR::decode_raw(raw[q], EX(q), EY(q), EZ(q), (float)wq(q), mf, ms, v01, v23);
-        const float pw = __fmul_rn(poly_q_omt(q, ux, uy, uz, omt), (float)wq(q));
-        float2 o01, o23, f01, f23;
-        collide_pairs(v01, v23, r01, r23, pw, c1a, c1b, c2a, c2b, (float)wq(q) * rt, o01, o23, f01, f23);
-        PR::store_pairs(Pout, q, ps, g, o01, o23, f01, f23);
-    }
-    if (b == 0 && j == 2 && (i == G.ia || i == G.ib)) {
-        T* Rcur = (T*)X.rcur;
-        Rcur[g] = rho;
-        Rcur[ps + g] = ca;
-        Rcur[2 * ps + g] = cb;
-        Rcur[3 * ps + g] = cc;
-    }
-    if (PR::kMoments) {
-        X.mcur[2 * (long long)g] = make_float4((float)rho, (float)ux, (float)uy, (float)uz);
-        X.mcur[2 * (long long)g + 1] = make_float4((float)ca, (float)cb, (float)cc, omt);
-    }
-    if (write_macro) {
-        double* Mac = X.mac;
-        Mac[g] = rho;
-        Mac[ps + g] = ux;
-        Mac[2 * ps + g] = uy;
-        Mac[3 * ps + g] = uz;
-        Mac[4 * ps + g] = ca;
-        Mac[5 * ps + g] = cb;
-        Mac[6 * ps + g] = cc;
-    }
+    const unsigned a = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(a), "l"(gmem) : "memory");
 }
 
 // One tile {mixer * 2 + box, x0 | y0 << 16, z0 | z1 << 16} (0-based x0, y0;
 // interior planes z0 .. z1-1, 2 <= z0 < z1 <= nz).  A and B hold the two
-// halves of 4 * (TY + 2) * 34 records.  TWO: the nodes take lp_interior_2p.
-// Every thread of the block runs the same iterations (the barriers are
-// uniform).
-template <class PR, int TY, bool TWO>
+// halves of 4 * (TY + 2) * 34 records.  With PF the populations are
+// pipelined too: each thread copies the 19 stored values its node of plane
+// k + 1 will read into its slots of PS (two planes of 19 x 32 TY values,
+// 8 bytes each) while it computes plane k, so the loads of both kinds are in
+// flight during the arithmetic.  Every thread of the block runs the same
+// iterations (the barriers are uniform).
+template <class PR, int TY, bool PF>
 __device__ __forceinline__ void sweep_tile(const StepPtrs& X, const Geom& G, const Phys& P, int write_macro, int4 t,
-                                           float4* A, float4* B)
+                                           float4* A, float4* B, typename PR::Raw* PS)
 {
     constexpr int RW = kSweepX + 2, PLANE = (TY + 2) * RW, NT = kSweepX * TY;
     const int b = t.x & 1;
@@ -844,7 +777,11 @@ __device__ __forceinline__ void sweep_tile(const StepPtrs& X, const Geom& G, con
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     const int nx = box_nx(G, b), ny = box_ny(G, b);
     const int x = x0 + tx, y = y0 + ty;
+    const bool in_box = x < nx && y < ny;
+    const int sy = nx, sz = nx * ny;
+    const int iface = (b == 0 && y == 0) ? 1 : ((b == 1 && y == G.mny - 1) ? 2 : 0);
     const float4* __restrict__ M = X.mprev;
+    const typename PR::S* __restrict__ Pin = (const typename PR::S*)X.pin;
     auto stage = [&](int kk) {
         const int slot = (kk & 3) * PLANE;
         for (int e = threadIdx.x; e < PLANE; e += NT) {
@@ -856,25 +793,41 @@ __device__ __forceinline__ void sweep_tile(const StepPtrs& X, const Geom& G, con
             }
         }
     };
+    // this thread's 19 stored values of plane kk (interior nodes only)
+    auto prefetch = [&](int kk) {
+        if (!in_box || is_boundary(G, b, x + 1, y + 1, kk)) return;
+        const int g = box_base(G, b) + ((kk - 1) * ny + y) * nx + x;
+        typename PR::Raw* dst = PS + (kk & 1) * 19 * NT + threadIdx.x;
+#pragma unroll
+        for (int q = 0; q < 19; q++) {
+            const int s = bulk_src(G, g, x + 1, kk, sy, sz, iface, q);
+            cp_async8(dst + q * NT, Pin + PR::off(0, q, G.ps, s));
+        }
+    };
     stage(z0 - 1);
     stage(z0);
     stage(z0 + 1);
+    if constexpr (PF) prefetch(z0);
     cp_async_commit();
     cp_async_wait_all();
     __syncthreads();
     for (int k = z0; k < z1; k++) {
         // plane k + 2 goes to the slot of plane k - 2, which no thread reads
-        // any more (the barrier at the end of the previous iteration)
+        // any more (the barrier at the end of the previous iteration); the
+        // populations of plane k + 1 to the other half of PS, which this
+        // thread finished reading in the previous iteration
         if (k + 2 < z1 + 1) stage(k + 2);
+        if constexpr (PF)
+            if (k + 1 < z1) prefetch(k + 1);
         cp_async_commit();
-        if (x < nx && y < ny && !is_boundary(G, b, x + 1, y + 1, k)) {
+        if (in_box && !is_boundary(G, b, x + 1, y + 1, k)) {
             const int g = box_base(G, b) + ((k - 1) * ny + y) * nx + x;
-            const RecShared<TY> rec{A, B, tx, ty, k};
-            if constexpr (TWO)
-                lp_interior_2p<PR, TY>(X, G, P, write_macro, g, b, x + 1, y + 1, k, rec);
+            if constexpr (PF)
+                lp_interior<PR>(X, G, P, write_macro, g, b, x + 1, y + 1, k, RecShared<TY>{A, B, tx, ty, k},
+                                PopStaged<PR>{PS + (k & 1) * 19 * NT + threadIdx.x, NT});
             else
-                lp_interior<PR>(X, G, P, write_macro, g, b, x + 1, y + 1, k, rec,
-                                PopGlobal<PR>{(const typename PR::S*)X.pin, G.ps});
+                lp_interior<PR>(X, G, P, write_macro, g, b, x + 1, y + 1, k, RecShared<TY>{A, B, tx, ty, k},
+                                PopGlobal<PR>{Pin, G.ps});
         }
         cp_async_wait_all();
         __syncthreads();
@@ -1703,18 +1656,23 @@ __device__ __forceinline__ void bulk_any(const StepPtrs& X, const Geom& G, const
     }
 
 // The FP16 form's interior as tiles (sweep_tile), persistent over the tile
-// list: 32 x 8 threads (two blocks per SM) or 32 x 4 (four) taking the
-// one-pass node, and the two-pass node at 32 x 4 (five blocks per SM) or
-// 32 x 8 (three).  Dynamic shared memory: sweep_smem_host(TY).
-#define TMX_SWEEP_KERNEL(PR, NAME, TY, TWO, SUFFIX, MINB)                                                         \
+// list: 32 x 8 threads (two blocks per SM) or 32 x 4 (four), and with the
+// populations pipelined 32 x 4 (three) or 32 x 2 (six).  The pipelined
+// 32 x 4 kernel takes its 65,024 bytes of shared memory dynamically.
+constexpr int sweep_smem_bytes(int ty, bool pf)
+{
+    return 2 * 4 * (ty + 2) * (kSweepX + 2) * 16 + (pf ? 2 * 19 * kSweepX * ty * 8 : 0);
+}
+#define TMX_SWEEP_KERNEL(PR, NAME, TY, PF, SUFFIX, MINB)                                                          \
     __global__ void __launch_bounds__(kSweepX * TY, MINB) k_sweep##SUFFIX##_##NAME(                              \
         StepPtrs X, Geom G, Phys P, int write_macro, const int4* __restrict__ tiles, int ntiles)                 \
     {                                                                                                           \
         extern __shared__ float4 sweep_smem[];                                                                  \
         float4* A = sweep_smem;                                                                                 \
         float4* B = A + 4 * (TY + 2) * (kSweepX + 2);                                                           \
+        PR::Raw* PS = (PR::Raw*)(B + 4 * (TY + 2) * (kSweepX + 2));                                             \
         for (int t = blockIdx.x; t < ntiles; t += gridDim.x)                                                    \
-            sweep_tile<PR, TY, TWO>(X, G, P, write_macro, tiles[t], A, B);                                      \
+            sweep_tile<PR, TY, PF>(X, G, P, write_macro, tiles[t], A, B, PS);                                   \
     }                                                                                                           \
     __global__ void __launch_bounds__(kSweepX * TY, MINB) k_sweep_batch##SUFFIX##_##NAME(                        \
         const MixerDesc* __restrict__ D, const int4* __restrict__ tiles, const int* __restrict__ counts,         \
@@ -1723,18 +1681,19 @@ __device__ __forceinline__ void bulk_any(const StepPtrs& X, const Geom& G, const
         extern __shared__ float4 sweep_smem[];                                                                  \
         float4* A = sweep_smem;                                                                                 \
         float4* B = A + 4 * (TY + 2) * (kSweepX + 2);                                                           \
+        PR::Raw* PS = (PR::Raw*)(B + 4 * (TY + 2) * (kSweepX + 2));                                             \
         const int n = counts[3];                                                                                \
         for (int t = blockIdx.x; t < n; t += gridDim.x) {                                                       \
             const int4 tl = tiles[t];                                                                           \
             const MixerDesc& d = D[tl.x >> 1];                                                                  \
-            sweep_tile<PR, TY, TWO>(d.X[parity], d.G, d.P, write_macro, tl, A, B);                              \
+            sweep_tile<PR, TY, PF>(d.X[parity], d.G, d.P, write_macro, tl, A, B, PS);                           \
         }                                                                                                       \
     }
 #define TMX_DEFINE_SWEEP_KERNELS(PR, NAME)        \
     TMX_SWEEP_KERNEL(PR, NAME, 8, false, 8, 2)    \
     TMX_SWEEP_KERNEL(PR, NAME, 4, false, 4, 4)    \
-    TMX_SWEEP_KERNEL(PR, NAME, 4, true, 4l, 5)    \
-    TMX_SWEEP_KERNEL(PR, NAME, 8, true, 8l, 3)
+    TMX_SWEEP_KERNEL(PR, NAME, 4, true, 4p, 3)    \
+    TMX_SWEEP_KERNEL(PR, NAME, 2, true, 2p, 6)
 
 // The face and the edge list as two launches (the FP32 and FP16-storage steps;
 // the FP64 step uses k_bound and k_walls).
