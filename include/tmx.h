@@ -244,16 +244,11 @@ int tmx_time_steps(tmx_handle *h, int nsteps, double *ms);
  * range (every form; zchunk ignored).  The sweep shapes (FP16 form only):
  * blocks of 32 x TY threads own tiles of as many nodes of one box and walk
  * them through zchunk planes (zchunk >= 1), the writers' moment records
- * staged in shared memory: TMX_SHAPE_SWEEP8 (TY 8), TMX_SHAPE_SWEEP4 (TY 4);
- * TMX_SHAPE_SWEEP4P / TMX_SHAPE_SWEEP2P (TY 4 / 2) also copy each node's
- * stored populations of the next plane into shared memory while the current
- * plane is computed.  Every shape gives the same results bit for bit.
- * Default: TMX_SHAPE_FLAT. */
+ * staged in shared memory: TMX_SHAPE_SWEEP8 (TY 8), TMX_SHAPE_SWEEP4 (TY 4).
+ * Every shape gives the same results bit for bit.  Default: TMX_SHAPE_FLAT. */
 #define TMX_SHAPE_FLAT 0
 #define TMX_SHAPE_SWEEP8 1
 #define TMX_SHAPE_SWEEP4 2
-#define TMX_SHAPE_SWEEP4P 3
-#define TMX_SHAPE_SWEEP2P 4
 int tmx_set_shape(tmx_handle *h, int kind, int zchunk);
 
 /* Node counts: out[0] fluid nodes (both boxes), out[1] interior nodes,

@@ -125,7 +125,7 @@ def test_wrong_precision_rejected(gpu):
 
 
 @pytest.mark.parametrize("kind,zchunk", [(T.SHAPE_SWEEP8, 3), (T.SHAPE_SWEEP4, 1), (T.SHAPE_SWEEP8, 64),
-                                         (T.SHAPE_SWEEP4P, 4), (T.SHAPE_SWEEP2P, 64)])
+                                         (T.SHAPE_SWEEP4, 16)])
 def test_sweep_shapes_agree(gpu, kind, zchunk):
     """The FP16 form's sweep interior kernel in a batch (tiles of every mixer
     in one list) gives each mixer its solo run's bits."""

@@ -390,8 +390,7 @@ class Solver:
 
     def set_shape(self, kind: int, zchunk: int = 8) -> "Solver":
         """Launch shape of the interior kernel (tmx_set_shape): SHAPE_FLAT, or
-        for the FP16 form a sweep shape (SHAPE_SWEEP8, SHAPE_SWEEP4, and with
-        the populations prefetched SHAPE_SWEEP4P, SHAPE_SWEEP2P) with zchunk
+        for the FP16 form a sweep shape (SHAPE_SWEEP8, SHAPE_SWEEP4) with zchunk
         planes per tile.  Every shape gives the same bits."""
         _check(lib().tmx_set_shape(self._h, int(kind), int(zchunk)))
         return self
@@ -564,9 +563,8 @@ class Request:
                          float(self.tol))
 
 
-SHAPE_FLAT, SHAPE_SWEEP8, SHAPE_SWEEP4, SHAPE_SWEEP4P, SHAPE_SWEEP2P = 0, 1, 2, 3, 4
-SHAPE_NAMES = {SHAPE_FLAT: "flat", SHAPE_SWEEP8: "sweep8", SHAPE_SWEEP4: "sweep4", SHAPE_SWEEP4P: "sweep4p",
-               SHAPE_SWEEP2P: "sweep2p"}
+SHAPE_FLAT, SHAPE_SWEEP8, SHAPE_SWEEP4 = 0, 1, 2
+SHAPE_NAMES = {SHAPE_FLAT: "flat", SHAPE_SWEEP8: "sweep8", SHAPE_SWEEP4: "sweep4"}
 SHAPE_KINDS = {v: k for k, v in SHAPE_NAMES.items()}
 
 SERVE_STATUS = {0: "converged", 1: "max_steps", -2: "too large for the budget", -5: "non-finite"}
@@ -663,5 +661,5 @@ def serve_with(engine, requests, check_every: int = 100, max_active: int = 0):
     return _serve_out(reqs, res[:len(reqs)], summ)
 
 
-__all__ = ["SHAPE_FLAT", "SHAPE_SWEEP8", "SHAPE_SWEEP4", "SHAPE_SWEEP4P", "SHAPE_SWEEP2P", "CaseSpec", "Solver", "Batch", "Request", "serve", "serve_with", "TmxError", "FIELDS", "TMX_FP64", "TMX_FP32", "TMX_FP16", "PRECISIONS",
+__all__ = ["SHAPE_FLAT", "SHAPE_SWEEP8", "SHAPE_SWEEP4", "CaseSpec", "Solver", "Batch", "Request", "serve", "serve_with", "TmxError", "FIELDS", "TMX_FP64", "TMX_FP32", "TMX_FP16", "PRECISIONS",
            "reference_case", "w_layout", "lib"]

@@ -219,7 +219,7 @@ struct tmx_batch {
     int zchunk = 8;      // planes per sweep tile
     int sms = 148;
     int grid_bulk[3] = {0, 0, 0};
-    int grid_sweep[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // by TMX_SHAPE_SWEEP* kind
+    int grid_sweep[4] = {0, 0, 0, 0};  // by TMX_SHAPE_SWEEP* kind
     int grid_faces = 0, grid_edges = 0;
     int nblocks = 0, nfaces = 0, nedges = 0, ntiles = 0, nactive = 0;
     cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
@@ -400,7 +400,7 @@ void set_grids(tmx_batch* b)
         b->grid_bulk[v] = b->sms * std::max(1, per);
     }
     if (b->K->moments && sweep_allow_smem() == cudaSuccess)
-        for (int kind = TMX_SHAPE_SWEEP8; kind <= TMX_SHAPE_SWEEP2P; kind++) {
+        for (int kind = TMX_SHAPE_SWEEP8; kind <= TMX_SHAPE_SWEEP4; kind++) {
             const SweepShape* sh = sweep_shape(kind);
             int per = 1;
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void*)sh->batch, sh->threads(), sh->smem());
@@ -895,7 +895,7 @@ int tmx_batch_tune(tmx_batch* b, int steps_per_trial, int* threads_out, int* cel
             }
         }
     if (b->K->moments)
-        for (int kind = TMX_SHAPE_SWEEP8; kind <= TMX_SHAPE_SWEEP2P; kind++)
+        for (int kind = TMX_SHAPE_SWEEP8; kind <= TMX_SHAPE_SWEEP4; kind++)
             for (int zi = 0; zi < 4 && rc == TMX_OK; zi++) {
                 rc = tmx_batch_set_sweep(b, kind, kZChunkChoices[zi]);
                 if (rc) break;

@@ -607,23 +607,14 @@ struct RecShared {
     }
 };
 
-// The stored populations of a source for lp_interior: loaded from global
-// memory (the flat bulk kernel and the sweep kernels without prefetch) ...
+// The stored populations of a source for lp_interior, loaded from global
+// memory.
 template <class PR>
 struct PopGlobal {
     const typename PR::S* __restrict__ Pin;
     long long ps;
     __device__ __forceinline__ typename PR::Raw operator()(int q, int s) const { return PR::load_raw(Pin, ps, q, s); }
 };
-// ... or from the copy a sweep kernel prefetched into shared memory for this
-// thread: direction q at base[q * stride].
-template <class PR>
-struct PopStaged {
-    const typename PR::Raw* base;
-    int stride;
-    __device__ __forceinline__ typename PR::Raw operator()(int q, int) const { return base[q * stride]; }
-};
-
 // One interior node (b, i, j, k) = g for the reduced-precision forms (FP32
 // arithmetic): every source index and (FP16 form) every writer's record
 // (from rec) is fetched once per direction and all 76 populations decoded in
@@ -753,23 +744,13 @@ __device__ __forceinline__ int tile_rec_node(const Geom& G, int b, int x, int y,
     return -1;
 }
 
-__device__ __forceinline__ void cp_async8(void* smem, const void* gmem)
-{
-    const unsigned a = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(a), "l"(gmem) : "memory");
-}
-
 // One tile {mixer * 2 + box, x0 | y0 << 16, z0 | z1 << 16} (0-based x0, y0;
 // interior planes z0 .. z1-1, 2 <= z0 < z1 <= nz).  A and B hold the two
-// halves of 4 * (TY + 2) * 34 records.  With PF the populations are
-// pipelined too: each thread copies the 19 stored values its node of plane
-// k + 1 will read into its slots of PS (two planes of 19 x 32 TY values,
-// 8 bytes each) while it computes plane k, so the loads of both kinds are in
-// flight during the arithmetic.  Every thread of the block runs the same
-// iterations (the barriers are uniform).
-template <class PR, int TY, bool PF>
+// halves of 4 * (TY + 2) * 34 records.  Every thread of the block runs the
+// same iterations (the barriers are uniform).
+template <class PR, int TY>
 __device__ __forceinline__ void sweep_tile(const StepPtrs& X, const Geom& G, const Phys& P, int write_macro, int4 t,
-                                           float4* A, float4* B, typename PR::Raw* PS)
+                                           float4* A, float4* B)
 {
     constexpr int RW = kSweepX + 2, PLANE = (TY + 2) * RW, NT = kSweepX * TY;
     const int b = t.x & 1;
@@ -777,11 +758,7 @@ __device__ __forceinline__ void sweep_tile(const StepPtrs& X, const Geom& G, con
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     const int nx = box_nx(G, b), ny = box_ny(G, b);
     const int x = x0 + tx, y = y0 + ty;
-    const bool in_box = x < nx && y < ny;
-    const int sy = nx, sz = nx * ny;
-    const int iface = (b == 0 && y == 0) ? 1 : ((b == 1 && y == G.mny - 1) ? 2 : 0);
     const float4* __restrict__ M = X.mprev;
-    const typename PR::S* __restrict__ Pin = (const typename PR::S*)X.pin;
     auto stage = [&](int kk) {
         const int slot = (kk & 3) * PLANE;
         for (int e = threadIdx.x; e < PLANE; e += NT) {
@@ -793,42 +770,20 @@ __device__ __forceinline__ void sweep_tile(const StepPtrs& X, const Geom& G, con
             }
         }
     };
-    // this thread's 19 stored values of plane kk (interior nodes only)
-    auto prefetch = [&](int kk) {
-        if (!in_box || is_boundary(G, b, x + 1, y + 1, kk)) return;
-        const int g = box_base(G, b) + ((kk - 1) * ny + y) * nx + x;
-        typename PR::Raw* dst = PS + (kk & 1) * 19 * NT + threadIdx.x;
-#pragma unroll
-        for (int q = 0; q < 19; q++) {
-            const int s = bulk_src(G, g, x + 1, kk, sy, sz, iface, q);
-            cp_async8(dst + q * NT, Pin + PR::off(0, q, G.ps, s));
-        }
-    };
     stage(z0 - 1);
     stage(z0);
     stage(z0 + 1);
-    if constexpr (PF) prefetch(z0);
     cp_async_commit();
     cp_async_wait_all();
     __syncthreads();
     for (int k = z0; k < z1; k++) {
         // plane k + 2 goes to the slot of plane k - 2, which no thread reads
-        // any more (the barrier at the end of the previous iteration); the
-        // populations of plane k + 1 to the other half of PS, which this
-        // thread finished reading in the previous iteration
+        // any more (the barrier at the end of the previous iteration)
         if (k + 2 < z1 + 1) stage(k + 2);
-        if constexpr (PF)
-            if (k + 1 < z1) prefetch(k + 1);
         cp_async_commit();
-        if (in_box && !is_boundary(G, b, x + 1, y + 1, k)) {
-            const int g = box_base(G, b) + ((k - 1) * ny + y) * nx + x;
-            if constexpr (PF)
-                lp_interior<PR>(X, G, P, write_macro, g, b, x + 1, y + 1, k, RecShared<TY>{A, B, tx, ty, k},
-                                PopStaged<PR>{PS + (k & 1) * 19 * NT + threadIdx.x, NT});
-            else
-                lp_interior<PR>(X, G, P, write_macro, g, b, x + 1, y + 1, k, RecShared<TY>{A, B, tx, ty, k},
-                                PopGlobal<PR>{Pin, G.ps});
-        }
+        if (x < nx && y < ny && !is_boundary(G, b, x + 1, y + 1, k))
+            lp_interior<PR>(X, G, P, write_macro, box_base(G, b) + ((k - 1) * ny + y) * nx + x, b, x + 1, y + 1, k,
+                            RecShared<TY>{A, B, tx, ty, k}, PopGlobal<PR>{(const typename PR::S*)X.pin, G.ps});
         cp_async_wait_all();
         __syncthreads();
     }
@@ -1656,44 +1611,34 @@ __device__ __forceinline__ void bulk_any(const StepPtrs& X, const Geom& G, const
     }
 
 // The FP16 form's interior as tiles (sweep_tile), persistent over the tile
-// list: 32 x 8 threads (two blocks per SM) or 32 x 4 (four), and with the
-// populations pipelined 32 x 4 (three) or 32 x 2 (six).  The pipelined
-// 32 x 4 kernel takes its 65,024 bytes of shared memory dynamically.
-constexpr int sweep_smem_bytes(int ty, bool pf)
-{
-    return 2 * 4 * (ty + 2) * (kSweepX + 2) * 16 + (pf ? 2 * 19 * kSweepX * ty * 8 : 0);
-}
-#define TMX_SWEEP_KERNEL(PR, NAME, TY, PF, SUFFIX, MINB)                                                          \
-    __global__ void __launch_bounds__(kSweepX * TY, MINB) k_sweep##SUFFIX##_##NAME(                              \
+// list: 32 x 8 threads (two blocks per SM) or 32 x 4 (four).  Dynamic shared
+// memory: sweep_smem_host(TY).
+#define TMX_SWEEP_KERNEL(PR, NAME, TY, MINB)                                                                      \
+    __global__ void __launch_bounds__(kSweepX * TY, MINB) k_sweep##TY##_##NAME(                                  \
         StepPtrs X, Geom G, Phys P, int write_macro, const int4* __restrict__ tiles, int ntiles)                 \
     {                                                                                                           \
         extern __shared__ float4 sweep_smem[];                                                                  \
         float4* A = sweep_smem;                                                                                 \
         float4* B = A + 4 * (TY + 2) * (kSweepX + 2);                                                           \
-        PR::Raw* PS = (PR::Raw*)(B + 4 * (TY + 2) * (kSweepX + 2));                                             \
-        for (int t = blockIdx.x; t < ntiles; t += gridDim.x)                                                    \
-            sweep_tile<PR, TY, PF>(X, G, P, write_macro, tiles[t], A, B, PS);                                   \
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x) sweep_tile<PR, TY>(X, G, P, write_macro, tiles[t], A, B); \
     }                                                                                                           \
-    __global__ void __launch_bounds__(kSweepX * TY, MINB) k_sweep_batch##SUFFIX##_##NAME(                        \
+    __global__ void __launch_bounds__(kSweepX * TY, MINB) k_sweep_batch##TY##_##NAME(                            \
         const MixerDesc* __restrict__ D, const int4* __restrict__ tiles, const int* __restrict__ counts,         \
         int parity, int write_macro)                                                                            \
     {                                                                                                           \
         extern __shared__ float4 sweep_smem[];                                                                  \
         float4* A = sweep_smem;                                                                                 \
         float4* B = A + 4 * (TY + 2) * (kSweepX + 2);                                                           \
-        PR::Raw* PS = (PR::Raw*)(B + 4 * (TY + 2) * (kSweepX + 2));                                             \
         const int n = counts[3];                                                                                \
         for (int t = blockIdx.x; t < n; t += gridDim.x) {                                                       \
             const int4 tl = tiles[t];                                                                           \
             const MixerDesc& d = D[tl.x >> 1];                                                                  \
-            sweep_tile<PR, TY, PF>(d.X[parity], d.G, d.P, write_macro, tl, A, B, PS);                           \
+            sweep_tile<PR, TY>(d.X[parity], d.G, d.P, write_macro, tl, A, B);                                   \
         }                                                                                                       \
     }
-#define TMX_DEFINE_SWEEP_KERNELS(PR, NAME)        \
-    TMX_SWEEP_KERNEL(PR, NAME, 8, false, 8, 2)    \
-    TMX_SWEEP_KERNEL(PR, NAME, 4, false, 4, 4)    \
-    TMX_SWEEP_KERNEL(PR, NAME, 4, true, 4p, 3)    \
-    TMX_SWEEP_KERNEL(PR, NAME, 2, true, 2p, 6)
+#define TMX_DEFINE_SWEEP_KERNELS(PR, NAME) \
+    TMX_SWEEP_KERNEL(PR, NAME, 8, 2)       \
+    TMX_SWEEP_KERNEL(PR, NAME, 4, 4)
 
 // The face and the edge list as two launches (the FP32 and FP16-storage steps;
 // the FP64 step uses k_bound and k_walls).

@@ -78,23 +78,20 @@ void inlet_scale(const tmx_case& c, const std::vector<double>& raw, double avera
                  std::vector<double>& U2);
 
 // The FP16 form's sweep kernels by shape (include/tmx.h TMX_SHAPE_SWEEP*):
-// tile height, population prefetch, the single-mixer and batched kernels and
-// their dynamic shared memory.
+// tile height, the single-mixer and batched kernels and their dynamic shared
+// memory.
 struct SweepShape {
     int kind, ty;
-    bool prefetch;
     void (*single)(tmx::StepPtrs, Geom, Phys, int, const int4*, int);
     void (*batch)(const tmx::MixerDesc*, const int4*, const int*, int, int);
     int threads() const { return 32 * ty; }
-    int smem() const { return tmx::sweep_smem_host(ty, prefetch); }
+    int smem() const { return tmx::sweep_smem_host(ty); }
 };
 inline const SweepShape* sweep_shape(int kind)
 {
     static const SweepShape shapes[] = {
-        {TMX_SHAPE_SWEEP8, 8, false, tmx::k_sweep8_f16, tmx::k_sweep_batch8_f16},
-        {TMX_SHAPE_SWEEP4, 4, false, tmx::k_sweep4_f16, tmx::k_sweep_batch4_f16},
-        {TMX_SHAPE_SWEEP4P, 4, true, tmx::k_sweep4p_f16, tmx::k_sweep_batch4p_f16},
-        {TMX_SHAPE_SWEEP2P, 2, true, tmx::k_sweep2p_f16, tmx::k_sweep_batch2p_f16},
+        {TMX_SHAPE_SWEEP8, 8, tmx::k_sweep8_f16, tmx::k_sweep_batch8_f16},
+        {TMX_SHAPE_SWEEP4, 4, tmx::k_sweep4_f16, tmx::k_sweep_batch4_f16},
     };
     for (const SweepShape& e : shapes)
         if (e.kind == kind) return &e;
@@ -104,7 +101,7 @@ inline const SweepShape* sweep_shape(int kind)
 // (idempotent); returns the first error.
 inline cudaError_t sweep_allow_smem()
 {
-    for (int kind = TMX_SHAPE_SWEEP8; kind <= TMX_SHAPE_SWEEP2P; kind++) {
+    for (int kind = TMX_SHAPE_SWEEP8; kind <= TMX_SHAPE_SWEEP4; kind++) {
         const SweepShape* sh = sweep_shape(kind);
         cudaError_t e = cudaFuncSetAttribute((const void*)sh->single, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              sh->smem());

@@ -79,8 +79,7 @@ TMX_DECLARE_BATCH_KERNELS(f16)
 // The FP16 form's interior by tiles of 32 x TY nodes swept through z
 // (tmx_engine.cuh sweep_tile): tiles[t] = {mixer * 2 + box, x0 | y0 << 16,
 // z0 | z1 << 16}; the single-mixer kernels take mixer 0, the batched ones read
-// the tile count from counts[3].  Suffix: TY, and "p" where the populations
-// are prefetched too.  Dynamic shared memory: sweep_smem_bytes(TY, prefetch).
+// the tile count from counts[3].  Dynamic shared memory: sweep_smem_host(TY).
 #define TMX_DECLARE_SWEEP(SUFFIX)                                                                               \
     __global__ void k_sweep##SUFFIX##_f16(StepPtrs X, Geom G, Phys P, int write_macro, const int4* tiles,     \
                                           int ntiles);                                                        \
@@ -88,12 +87,7 @@ TMX_DECLARE_BATCH_KERNELS(f16)
                                                 int parity, int write_macro);
 TMX_DECLARE_SWEEP(8)
 TMX_DECLARE_SWEEP(4)
-TMX_DECLARE_SWEEP(4p)
-TMX_DECLARE_SWEEP(2p)
-constexpr int sweep_smem_host(int ty, bool pf)
-{
-    return 2 * 4 * (ty + 2) * 34 * 16 + (pf ? 2 * 19 * 32 * ty * 8 : 0);
-}
+constexpr int sweep_smem_host(int ty) { return 2 * 4 * (ty + 2) * 34 * 16; }
 
 // Outlet mixing quality of batch mixers: for entry e, mixer slots[e], the
 // I_A, I_B, I_C of mixing row 1 (the first row of tmx_mixing) into
