@@ -488,7 +488,16 @@ def run_batched(args, dist: Dist, fp64_mlups: float, peaks: dict) -> dict:
     with T.Batch(T.TMX_FP16, budget=budget, device=dist.local_rank) as B:
         for s in specs:
             B.add(s)
-        tuned = B.tune(steps_per_trial=20)
+        if args.batched_shape:
+            # a fixed interior kernel instead of the autotuner (profiling)
+            kind, z = args.batched_shape.split(":")
+            if kind == "flat":
+                B.set_shape(256, int(z))
+            else:
+                B.set_sweep(T.SHAPE_KINDS[kind], int(z))
+            tuned = dict(B.shape(), ms_per_step=None, steps_per_trial=0, fixed=args.batched_shape)
+        else:
+            tuned = B.tune(steps_per_trial=20)
         B.step(args.warmup, write_macro=False)
         B.sync()
         ms = B.time_steps(args.batched_steps)
@@ -592,6 +601,9 @@ def main(argv=None) -> int:
     ap.add_argument("--batched-mixers", type=int, default=64)
     ap.add_argument("--batched-steps", type=int, default=5000)
     ap.add_argument("--served-requests", type=int, default=64)
+    ap.add_argument("--batched-shape", default=None,
+                    help="fix the batched interior kernel instead of autotuning: flat:CELLS or sweep4:PLANES / "
+                         "sweep8:PLANES")
     ap.add_argument("--served-max-steps", type=int, default=50000)
 
     args = ap.parse_args(argv)
