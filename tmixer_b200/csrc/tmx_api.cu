@@ -76,6 +76,9 @@ struct tmx_handle {
     cudaEvent_t fork = nullptr, join = nullptr, join2 = nullptr;
     int nface = 0;  // the first nface boundary nodes are face classes
     int nwall = 0;  // the last nwall are wall faces (StepKernels::walls)
+    // FP32 / FP16 forms: the last nzwall faces are the z wall faces, which
+    // the sweep kernels update (boundary_list)
+    int nzwall = 0;
     // one captured step per (state buffer, macroscopic output) combination
     cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
     int sbytes = 8, tbytes = 8;  // storage / arithmetic bytes per value of the form
@@ -330,33 +333,63 @@ void inlet_profile(const tmx_case& c, std::vector<double>& U1, std::vector<doubl
 }
 
 int boundary_list(const Geom& G, std::vector<int>& nodes, std::vector<unsigned char>& cls, int& nface,
-                  std::vector<int>* class_count, int* nwall)
+                  std::vector<int>* class_count, int* nwall, int* nzwall)
 {
-    std::vector<std::pair<int, int>> bl;
-    bl.reserve((size_t)boundary_count(G));
+    struct Entry {
+        int cls, wall, node;
+        bool zwall;
+    };
+    std::vector<Entry> all;
+    all.reserve((size_t)boundary_count(G));
     if (class_count) class_count->assign(tmx::K_NCLASSES, 0);
+    bool zsep = nzwall != nullptr && nwall == nullptr;
+    long long zcount = 0, interior2 = 0;
     for (int b = 0; b < 2; b++)
         for (int i = 1; i <= G.nx[b]; i++)
-            for (int j = 1; j <= G.ny[b]; j++)
+            for (int j = 1; j <= G.ny[b]; j++) {
+                if (G.nz >= 3 && !tmx::is_boundary(G, b, i, j, 2)) interior2++;
                 for (int k = 1; k <= G.nz; k++) {
                     if (!tmx::is_boundary(G, b, i, j, k)) continue;
                     const int c = classify(G, b, i, j, k);
-                    if (c < 0) return fail(TMX_E_INVALID, "internal: boundary node (%d,%d,%d,%d) has no class", b, i, j, k);
+                    if (c < 0)
+                        return fail(TMX_E_INVALID, "internal: boundary node (%d,%d,%d,%d) has no class", b, i, j, k);
                     const int w = tmx::wall_class(G, b, i, j, k);
                     if (w != (tmx::is_wall_class(c) ? c : -1))
                         return fail(TMX_E_INVALID, "internal: wall class %d of node (%d,%d,%d,%d), class %d", w, b, i,
                                     j, k, c);
                     if (class_count) (*class_count)[c]++;
-                    // faces first, then edges and corners (then, with nwall,
-                    // the wall faces); by class, then node
-                    const int key = (nwall && w >= 0) ? 512 : (tmx::is_face_class(c) ? 0 : 256) + c;
-                    bl.emplace_back(key, tmx::node_index(G, b, i, j, k));
+                    const bool zw = c == tmx::K_FACE_Z1 || c == tmx::K_FACE_ZT;
+                    if (zw) {
+                        // the interior node of the column the sweep kernels
+                        // update this wall node with (sweep_zwall)
+                        const int kw = c == tmx::K_FACE_Z1 ? 1 : G.nz, kn = c == tmx::K_FACE_Z1 ? 2 : G.nz - 1;
+                        if (k != kw || G.nz < 3 || tmx::is_boundary(G, b, i, j, kn)) zsep = false;
+                        zcount++;
+                    }
+                    all.push_back({c, w, tmx::node_index(G, b, i, j, k), zw});
                 }
+            }
+    // every z wall node above or below an interior node, and every interior
+    // node of planes 2 and nz - 1 under or over one
+    if (zcount != 2 * interior2) zsep = false;
+    if (nzwall && nwall == nullptr && !zsep && interior2 > 0)
+        return fail(TMX_E_INVALID, "internal: the z wall faces do not pair with the interior nodes of planes 2 and %d",
+                    G.nz - 1);
+    // faces first (with zsep the z wall faces last among them), then edges
+    // and corners (then, with nwall, the wall faces); by class, then node
+    std::vector<std::pair<int, int>> bl;
+    bl.reserve(all.size());
+    for (const Entry& e : all) {
+        const int key = (nwall && e.wall >= 0)
+                            ? 512
+                            : (tmx::is_face_class(e.cls) ? (zsep && e.zwall ? 128 : 0) : 256) + e.cls;
+        bl.emplace_back(key, e.node);
+    }
     std::sort(bl.begin(), bl.end());
     nodes.resize(bl.size());
     cls.resize(bl.size());
     nface = 0;
-    int nw = 0;
+    int nw = 0, nzw = 0;
     for (size_t t = 0; t < bl.size(); t++) {
         nodes[t] = bl[t].second;
         if (bl[t].first == 512) {  // the walls in node order
@@ -365,11 +398,13 @@ int boundary_list(const Geom& G, std::vector<int>& nodes, std::vector<unsigned c
             cls[t] = (unsigned char)tmx::wall_class(G, b, i, j, k);
             nw++;
         } else {
-            cls[t] = (unsigned char)(bl[t].first & 255);
+            cls[t] = (unsigned char)(bl[t].first & 127);
         }
         if (bl[t].first < 256) nface++;
+        if (bl[t].first >= 128 && bl[t].first < 256) nzw++;
     }
     if (nwall) *nwall = nw;
+    if (nzwall) *nzwall = nzw;
     return TMX_OK;
 }
 
@@ -451,8 +486,11 @@ int enqueue_step(tmx_handle* h, int cur, int write_macro, cudaEvent_t* ev)
             h->K->walls<<<(nw + bt - 1) / bt, bt, 0, h->aux2>>>(X, h->bnode + nf + ne, h->bcls + nf + ne, nw, G, h->P,
                                                                 write_macro);
     } else {
-        if (nf > 0)
-            h->K->faces<<<(nl * nf + bt - 1) / bt, bt, 0, h->aux>>>(X, h->bnode, h->bcls, nf, G, h->P, write_macro);
+        // with a sweep shape the interior kernel updates the z wall faces,
+        // the last nzwall of the face range (zwall_node)
+        const int nfk = sweep_shape(h->shape) ? nf - h->nzwall : nf;
+        if (nfk > 0)
+            h->K->faces<<<(nl * nfk + bt - 1) / bt, bt, 0, h->aux>>>(X, h->bnode, h->bcls, nfk, G, h->P, write_macro);
         if (ne > 0)
             h->K->edges<<<(nl * ne + bt - 1) / bt, bt, 0, h->aux2>>>(X, h->bnode + nf, h->bcls + nf, ne, G, h->P,
                                                                      write_macro);
@@ -690,7 +728,7 @@ int tmx_create(const tmx_case* c, int device, tmx_handle** out)
     // boundary node list, faces first, sorted by class then node index
     std::vector<int> nodes;
     std::vector<unsigned char> cls;
-    rc = boundary_list(G, nodes, cls, h->nface, &h->class_count, h->K->walls ? &h->nwall : nullptr);
+    rc = boundary_list(G, nodes, cls, h->nface, &h->class_count, h->K->walls ? &h->nwall : nullptr, &h->nzwall);
     if (rc) {
         delete h;
         return rc;

@@ -8,7 +8,9 @@
 //     {mixer, first node, node count}; the boundary kernels walk the
 //     concatenated face and edge node lists {node, mixer * 256 + class}.  A
 //     mixer's descriptor (buffers per step parity, geometry, physics) is
-//     read by the kernels from device memory.
+//     read from device memory; the sweep and boundary kernels copy it into
+//     shared memory once per tile or per 32 list entries (the lists are
+//     padded so that those belong to one mixer).
 //   - Step parity: a batch-wide counter; a mixer admitted when the counter's
 //     parity is p reads its initial buffer at parity p (the descriptor's two
 //     buffer sets are swapped accordingly), so mixers of different ages step
@@ -95,6 +97,7 @@ struct Slot {
     std::vector<int> nodes;
     std::vector<unsigned char> cls;
     int nface = 0;
+    int nzwall = 0;  // z wall faces last among the faces (boundary_list)
     int parity0 = 0;  // batch parity at admission
     long long steps = 0;
 };
@@ -297,13 +300,22 @@ int rebuild(tmx_batch* b)
         for (int g0 = 0; g0 < s.G.nnodes; g0 += b->cells)
             blocks.push_back(make_int4((int)m, g0, std::min(b->cells, s.G.nnodes - g0), 0));
         if (b->sweep) sweep_tiles(s.G, (int)m, sweep_shape(b->sweep)->ty, b->zchunk, tiles);
+        // with a sweep shape the interior kernel updates the z wall faces,
+        // the last nzwall of the face range (zwall_node)
+        const int nfk = b->sweep ? s.nface - s.nzwall : s.nface;
         for (size_t t = 0; t < s.nodes.size(); t++) {
             const int2 e = make_int2(s.nodes[t], (int)m * 256 + s.cls[t]);
-            if ((int)t < s.nface)
-                faces.push_back(e);
-            else
+            if ((int)t < s.nface) {
+                if ((int)t < nfk) faces.push_back(e);
+            } else {
                 edges.push_back(e);
+            }
         }
+        // each mixer's entries start at a multiple of kListAlign, so that
+        // the kListAlign entries a block takes at a time belong to one mixer
+        const int2 pad = make_int2(-1, (int)m * 256);
+        while (faces.size() % tmx::kListAlign) faces.push_back(pad);
+        while (edges.size() % tmx::kListAlign) edges.push_back(pad);
     }
     cudaError_t e = grow(b, b->d_desc, b->cap_desc, (int)std::max<size_t>(1, desc.size()));
     if (e == cudaSuccess) e = grow(b, b->d_blocks, b->cap_blocks, (int)std::max<size_t>(1, blocks.size()));
@@ -549,7 +561,7 @@ int admit(tmx_batch* b, const tmx_case* c, const void* buf, long long size, int*
     if (off < 0)
         return fail(TMX_E_NOMEM, "batch budget: %lld bytes needed, %lld free (largest range %lld)", cv.total,
                     b->arena.free_bytes(), b->arena.largest());
-    rc = boundary_list(s.G, s.nodes, s.cls, s.nface, nullptr, nullptr);
+    rc = boundary_list(s.G, s.nodes, s.cls, s.nface, nullptr, nullptr, &s.nzwall);
     if (rc) {
         b->arena.release(off, cv.total);
         return rc;

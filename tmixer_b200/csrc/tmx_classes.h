@@ -44,6 +44,8 @@ enum BoundaryClass : unsigned char {
     K_JUNC_CC,           // edge CC' (:8793): inlet x=ib, y=1
     K_NCLASSES
 };
+// the host's sort keys of the boundary lists hold a class in 7 bits
+static_assert(K_NCLASSES <= 128, "class fits the list sort key");
 
 // Inlets, outlet and wall faces (one kernel); edges and corners (the other).
 __host__ __device__ constexpr bool is_face_class(int c)

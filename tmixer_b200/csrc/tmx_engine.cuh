@@ -293,7 +293,6 @@ struct F16 {
     // value is one multiply
     __device__ static void poly(T ux, T uy, T uz, T (&p)[19])
     {
-#pragma unroll
         const float omt = omt_term(ux, uy, uz);
 #pragma unroll
         for (int q = 0; q < 19; q++) p[q] = __fmul_rn(poly_q_omt(q, ux, uy, uz, omt), (float)wq(q));
@@ -626,7 +625,6 @@ __device__ __forceinline__ void lp_interior(const StepPtrs& X, const Geom& G, co
                                             int b, int i, int j, int k, const Rec& rec, const Pop& pop)
 {
     using T = typename PR::T;
-    const typename PR::S* __restrict__ Pin = (const typename PR::S*)X.pin;
     typename PR::S* __restrict__ Pout = (typename PR::S*)X.pout;
     const long long ps = G.ps;
     const int sy = box_nx(G, b), sz = box_nx(G, b) * box_ny(G, b);
@@ -692,6 +690,99 @@ __device__ __forceinline__ void lp_interior(const StepPtrs& X, const Geom& G, co
 }
 
 
+template <class T>
+__device__ __forceinline__ void wall_flow_closure(int cls, T rout, T (&v)[19]);
+
+// The z wall face node (b, i, j, kw), kw = 1 or nz (class K_FACE_Z1 or
+// K_FACE_ZT), above or below interior node (b, i, j, kn), kn = 2 or nz - 1,
+// which the calling thread of a sweep kernel has just updated.  Every z wall
+// face node lies over an interior node and every interior node of planes 2
+// and nz - 1 under one (boundary_list checks it), and with a sweep shape the
+// boundary lists leave these nodes to the sweep kernels.  The node's flow is pulled from planes kw and kn
+// and closed by the wall closure; its species are the interior neighbour's
+// pulls (the zero-gradient copy).  The operations are those of
+// boundary_lane_lp's four lanes for these classes (decode_raw, the closure,
+// sum19, momentum, pw_dir, collide_dir), so the results equal the face
+// kernel's bit for bit.  recw / recn give the writers' records of the wall
+// node's and of the interior node's sources (FP16 form).
+template <class PR, class Rec>
+__device__ __forceinline__ void zwall_node(const StepPtrs& X, const Geom& G, const Phys& P, int write_macro, int b,
+                                           int i, int j, int kw, int kn, int gw, int gn, const Rec& recw,
+                                           const Rec& recn)
+{
+    using T = typename PR::T;
+    const typename PR::S* __restrict__ Pin = (const typename PR::S*)X.pin;
+    typename PR::S* __restrict__ Pout = (typename PR::S*)X.pout;
+    const long long ps = G.ps;
+    const int sy = box_nx(G, b), sz = box_nx(G, b) * box_ny(G, b);
+    const int iface = (b == 0 && j == 1) ? 1 : ((b == 1 && j == G.mny) ? 2 : 0);
+    const int dz = kw == 1 ? 1 : -1;  // the lattice z component of the unknown directions
+    const PopGlobal<PR> pop{Pin, ps};
+    T f[19], a[19], bb[19], cc[19];
+#pragma unroll
+    for (int q = 0; q < 19; q++) {
+        float4 mf = make_float4(0.f, 0.f, 0.f, 0.f), ms = mf;
+        float2 v01, v23;
+        const int s1 = bulk_src(G, gn, i, kn, sy, sz, iface, q);
+        if constexpr (PR::kMoments) recn(q, s1, mf, ms);
+        PR::decode_raw(pop(q, s1), EX(q), EY(q), EZ(q), (float)wq(q), mf, ms, v01, v23);
+        a[q] = v01.y;
+        bb[q] = v23.x;
+        cc[q] = v23.y;
+        f[q] = T(0);
+        if (EZ(q) != dz) {
+            const int s0 = bulk_src(G, gw, i, kw, sy, sz, iface, q);
+            if constexpr (PR::kMoments) recw(q, s0, mf, ms);
+            PR::decode_raw(pop(q, s0), EX(q), EY(q), EZ(q), (float)wq(q), mf, ms, v01, v23);
+            f[q] = v01.x;
+        }
+    }
+    wall_flow_closure(kw == 1 ? (int)K_FACE_Z1 : (int)K_FACE_ZT, T(P.rho_out), f);
+    const T rho = sum19(f), ca = sum19(a), cb = sum19(bb), ccc = sum19(cc);
+    T sxm, sym, szm;
+    momentum(f, sxm, sym, szm);
+    const T ux = sxm / rho, uy = sym / rho, uz = szm / rho;
+    const T rt = T(P.rateconst) * ca * cb;
+    const T rr[4] = {rho, ca, cb, ccc};
+    T c1[4], c2[4];
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+        c1[m] = T(P.c1[m]);
+        c2[m] = T(P.c2[m]);
+    }
+#pragma unroll
+    for (int q = 0; q < 19; q++) {
+        const T in[4] = {f[q], a[q], bb[q], cc[q]};
+        PR::collide_dir(Pout, q, ps, gw, in, rr, PR::pw_dir(EX(q), EY(q), EZ(q), (float)wq(q), ux, uy, uz), c1, c2,
+                        (float)wq(q), rt);
+    }
+    T* __restrict__ Rcur = (T*)X.rcur;
+    Rcur[gw] = rho;
+    Rcur[ps + gw] = ca;
+    Rcur[2 * ps + gw] = cb;
+    Rcur[3 * ps + gw] = ccc;
+    if constexpr (PR::kMoments) {
+        X.mcur[2 * (long long)gw] = make_float4((float)rho, (float)ux, (float)uy, (float)uz);
+        X.mcur[2 * (long long)gw + 1] =
+            make_float4((float)ca, (float)cb, (float)ccc, omt_term((float)ux, (float)uy, (float)uz));
+    }
+    if (write_macro) {
+        double* Mac = X.mac;
+        Mac[gw] = rho;
+        Mac[ps + gw] = ux;
+        Mac[2 * ps + gw] = uy;
+        Mac[3 * ps + gw] = uz;
+        Mac[4 * ps + gw] = ca;
+        Mac[5 * ps + gw] = cb;
+        Mac[6 * ps + gw] = ccc;
+    }
+}
+
+// One interior node of the FP32 / FP16 forms in the flat bulk kernels.  (The
+// z wall faces stay with the face kernel here: updated by these kernels as
+// well, the walls cost them registers (168 B of spills) and the 4-mixer FP16
+// batch step went from 571 to 680-697 us, the W=32 FP16 step from 69.2 to
+// 73.1 us.)
 template <class PR>
 __device__ __forceinline__ void bulk_node_lp(const StepPtrs& X, const Geom& G, const Phys& P, int write_macro, int g)
 {
@@ -747,7 +838,10 @@ __device__ __forceinline__ int tile_rec_node(const Geom& G, int b, int x, int y,
 // One tile {mixer * 2 + box, x0 | y0 << 16, z0 | z1 << 16} (0-based x0, y0;
 // interior planes z0 .. z1-1, 2 <= z0 < z1 <= nz).  A and B hold the two
 // halves of 4 * (TY + 2) * 34 records.  Every thread of the block runs the
-// same iterations (the barriers are uniform).
+// same iterations (the barriers are uniform).  The tiles of the first chunk
+// (z0 = 2) also update the z = 1 wall face nodes of their columns, those of
+// the last chunk (z1 = nz) the z = nz ones (zwall_node), the records of
+// both planes being in the ring.
 template <class PR, int TY>
 __device__ __forceinline__ void sweep_tile(const StepPtrs& X, const Geom& G, const Phys& P, int write_macro, int4 t,
                                            float4* A, float4* B)
@@ -781,9 +875,17 @@ __device__ __forceinline__ void sweep_tile(const StepPtrs& X, const Geom& G, con
         // any more (the barrier at the end of the previous iteration)
         if (k + 2 < z1 + 1) stage(k + 2);
         cp_async_commit();
-        if (x < nx && y < ny && !is_boundary(G, b, x + 1, y + 1, k))
-            lp_interior<PR>(X, G, P, write_macro, box_base(G, b) + ((k - 1) * ny + y) * nx + x, b, x + 1, y + 1, k,
-                            RecShared<TY>{A, B, tx, ty, k}, PopGlobal<PR>{(const typename PR::S*)X.pin, G.ps});
+        if (x < nx && y < ny && !is_boundary(G, b, x + 1, y + 1, k)) {
+            const int g = box_base(G, b) + ((k - 1) * ny + y) * nx + x;
+            lp_interior<PR>(X, G, P, write_macro, g, b, x + 1, y + 1, k, RecShared<TY>{A, B, tx, ty, k},
+                            PopGlobal<PR>{(const typename PR::S*)X.pin, G.ps});
+            if (k == 2)
+                zwall_node<PR>(X, G, P, write_macro, b, x + 1, y + 1, 1, 2, g - nx * ny, g,
+                               RecShared<TY>{A, B, tx, ty, 1}, RecShared<TY>{A, B, tx, ty, 2});
+            if (k == G.nz - 1)
+                zwall_node<PR>(X, G, P, write_macro, b, x + 1, y + 1, G.nz, k, g + nx * ny, g,
+                               RecShared<TY>{A, B, tx, ty, G.nz}, RecShared<TY>{A, B, tx, ty, k});
+        }
         cp_async_wait_all();
         __syncthreads();
     }
@@ -1610,6 +1712,33 @@ __device__ __forceinline__ void bulk_any(const StepPtrs& X, const Geom& G, const
             bulk_any<PR>(X, G, P, write_macro, g);                                                              \
     }
 
+// A batched kernel's block works on one mixer at a time (a sweep tile, 32
+// entries of a boundary list).  The block copies what the step reads of that
+// mixer's descriptor (the buffers of this step's parity, the geometry, the
+// physics) to shared memory, between two barriers of the caller, and the
+// step code reads them from there: read through a reference into the global
+// descriptor array, the compiler reloaded them from global memory inside the
+// node loop (about 60 extra global loads per interior node of the sweep
+// kernel, which cost it 12% of its time).  The flat interior kernel keeps
+// the global descriptor: its two barriers per cell block cost more than the
+// reloads.
+struct StepDesc {
+    StepPtrs X;
+    Geom G;
+    Phys P;
+};
+__device__ __forceinline__ void load_desc(StepDesc& dst, const MixerDesc* __restrict__ D, int m, int parity)
+{
+    static_assert(sizeof(StepPtrs) % 8 == 0 && sizeof(Geom) % 8 == 0 && sizeof(Phys) % 8 == 0 &&
+                      sizeof(StepDesc) == sizeof(StepPtrs) + sizeof(Geom) + sizeof(Phys),
+                  "descriptor copied in 8-byte words");
+    constexpr int nx = sizeof(StepPtrs) / 8, nw = sizeof(StepDesc) / 8;
+    const unsigned long long* __restrict__ sx = (const unsigned long long*)&D[m].X[parity];
+    const unsigned long long* __restrict__ sg = (const unsigned long long*)&D[m].G;
+    unsigned long long* d = (unsigned long long*)&dst;
+    for (int e = threadIdx.x; e < nw; e += blockDim.x) d[e] = e < nx ? __ldg(sx + e) : __ldg(sg + (e - nx));
+}
+
 // The FP16 form's interior as tiles (sweep_tile), persistent over the tile
 // list: 32 x 8 threads (two blocks per SM) or 32 x 4 (four).  Dynamic shared
 // memory: sweep_smem_host(TY).
@@ -1629,11 +1758,14 @@ __device__ __forceinline__ void bulk_any(const StepPtrs& X, const Geom& G, const
         extern __shared__ float4 sweep_smem[];                                                                  \
         float4* A = sweep_smem;                                                                                 \
         float4* B = A + 4 * (TY + 2) * (kSweepX + 2);                                                           \
+        __shared__ StepDesc d;                                                                                  \
         const int n = counts[3];                                                                                \
         for (int t = blockIdx.x; t < n; t += gridDim.x) {                                                       \
             const int4 tl = tiles[t];                                                                           \
-            const MixerDesc& d = D[tl.x >> 1];                                                                  \
-            sweep_tile<PR, TY>(d.X[parity], d.G, d.P, write_macro, tl, A, B);                                   \
+            __syncthreads();                                                                                    \
+            load_desc(d, D, tl.x >> 1, parity);                                                                 \
+            __syncthreads();                                                                                    \
+            sweep_tile<PR, TY>(d.X, d.G, d.P, write_macro, tl, A, B);                                           \
         }                                                                                                       \
     }
 #define TMX_DEFINE_SWEEP_KERNELS(PR, NAME) \
@@ -1697,22 +1829,32 @@ __device__ __forceinline__ void bulk_any(const StepPtrs& X, const Geom& G, const
             for (int t = threadIdx.x; t < cb.z; t += NT) bulk_any<PR>(d.X[parity], d.G, d.P, write_macro, cb.y + t); \
         }                                                                                                       \
     }
+// The batched boundary kernels hold the shared descriptor's values in
+// registers; their register counts are held to those of the global-descriptor
+// build (72 and 80 for the interleaved forms' faces and edges, 128 for FP64),
+// which kept them at 7, 6 and 4 blocks per SM: the 4-mixer FP16 sweep step
+// took 511-517 us capped against 528-533 us uncapped.
 #define TMX_BOUNDARY_BATCH(PR, NAME, KIND, FACES, WHICH)                                                          \
-    __global__ void __launch_bounds__(kBoundaryThreads) k_##KIND##_batch_##NAME(                               \
+    __global__ void __launch_bounds__(kBoundaryThreads, PR::kOnePass ? (FACES ? 7 : 6) : 4)                    \
+        k_##KIND##_batch_##NAME(                                                                                \
         const MixerDesc* __restrict__ D, const int2* __restrict__ list, const int* __restrict__ counts,         \
         int parity, int write_macro)                                                                            \
     {                                                                                                           \
         const int n = counts[WHICH];                                                                            \
-        __shared__ PR::T buf[PR::kOnePass ? kBoundaryThreads / 4 : 1][76];                                                         \
+        __shared__ PR::T buf[PR::kOnePass ? kBoundaryThreads / 4 : 1][76];                                      \
+        __shared__ StepDesc d;                                                                                  \
         for (int base = blockIdx.x * blockDim.x; base < 4 * n; base += gridDim.x * blockDim.x) {                \
             const int t = (base + threadIdx.x) >> 2, fld = threadIdx.x & 3;                                     \
-            const unsigned mask = __ballot_sync(0xffffffffu, t < n);                                            \
-            if (t < n) {                                                                                        \
-                const int2 e = list[t];                                                                         \
-                const MixerDesc& d = D[e.y >> 8];                                                               \
-                boundary_any<PR, FACES>(d.X[parity], d.G, d.P, write_macro, e.x, e.y & 255, fld, mask,          \
+            /* entries base / 4 .. base / 4 + 31 belong to one mixer (kListAlign) */                            \
+            __syncthreads();                                                                                    \
+            load_desc(d, D, list[base >> 2].y >> 8, parity);                                                    \
+            __syncthreads();                                                                                    \
+            const int2 e = t < n ? list[t] : make_int2(-1, 0);                                                  \
+            const bool live = e.x >= 0;                                                                         \
+            const unsigned mask = __ballot_sync(0xffffffffu, live);                                             \
+            if (live)                                                                                           \
+                boundary_any<PR, FACES>(d.X, d.G, d.P, write_macro, e.x, e.y & 255, fld, mask,                  \
                                         (threadIdx.x & 31) & ~3, buf[threadIdx.x >> 2]);                        \
-            }                                                                                                   \
         }                                                                                                       \
     }
 #define TMX_DEFINE_BATCH_KERNELS(PR, NAME)        \

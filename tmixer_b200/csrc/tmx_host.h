@@ -60,9 +60,14 @@ int classify(const Geom& G, int b, int i, int j, int k);
 // Boundary nodes sorted faces first, then by class, then by node index; the
 // first nface entries are face classes.  With nwall the wall faces
 // (tmx::wall_class) come last, in node order, and *nwall counts them.
-// Returns TMX_OK or a failure code.
+// Without nwall and with nzwall (the FP32 and FP16 forms), the z wall faces
+// (K_FACE_Z1, K_FACE_ZT) come last among the faces and *nzwall counts them:
+// each lies above or below an interior node and each interior node of planes
+// 2 and nz - 1 has one (checked; an internal error otherwise), and the sweep
+// kernels update them (zwall_node).  Without interior nodes (nz < 3) they
+// stay in place and *nzwall is 0.  Returns TMX_OK or a failure code.
 int boundary_list(const Geom& G, std::vector<int>& nodes, std::vector<unsigned char>& cls, int& nface,
-                  std::vector<int>* class_count, int* nwall);
+                  std::vector<int>* class_count, int* nwall, int* nzwall);
 // Inlet profiles Uin1, Uin2 ((iny+3) x (nz+3)) as the reference computes them:
 // the duct series (which depends on iny and nz only) and its mean, then the
 // scaling to umean and the shifts.

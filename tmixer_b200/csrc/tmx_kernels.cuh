@@ -24,6 +24,9 @@ struct StepPtrs {
 
 constexpr int kBoundaryThreadsHost = 128;  // block size of the boundary kernels
 constexpr int kBoundaryLanesHost = 4;      // threads per boundary node (one per field)
+// A batched boundary block takes kListAlign consecutive list entries at a
+// time; the batch pads each mixer's part of a list to a multiple of it.
+constexpr int kListAlign = kBoundaryThreadsHost / kBoundaryLanesHost;
 
 #define TMX_DECLARE_STEP_KERNELS(NAME)                                                                          \
     __global__ void k_init_##NAME(StepPtrs X, Geom G, Phys P, double rho0);                                     \
@@ -57,7 +60,8 @@ struct MixerDesc {
 //   bulk    a persistent grid walks a list of cell blocks {mixer, first
 //           node, node count, 0}; NT threads per block (128, 256 or 512).
 //   faces / edges   boundary-node lists of {node, mixer * 256 + class},
-//           four threads per node, persistent grid.
+//           four threads per node, persistent grid; each mixer's part
+//           starts at a multiple of kListAlign, padded with node -1.
 // counts[0..2] = number of cell blocks, face nodes, edge nodes (device
 // memory, so that captured graphs stay valid when the batch changes).
 #define TMX_DECLARE_BATCH_KERNELS(NAME)                                                                           \
