@@ -220,6 +220,8 @@ struct tmx_batch {
     int cells = 4096;    // nodes per cell block
     int sweep = 0;       // 0: the flat kernel; else the TMX_SHAPE_SWEEP* shape of the interior
     int zchunk = 8;      // planes per sweep tile
+    int bound_bps = 0;   // boundary kernels' blocks per SM (0: as many as fit)
+    int bound_fit = 1;   // blocks of the face kernel that fit on an SM
     int sms = 148;
     int grid_bulk[3] = {0, 0, 0};
     int grid_sweep[4] = {0, 0, 0, 0};  // by TMX_SHAPE_SWEEP* kind
@@ -421,8 +423,12 @@ void set_grids(tmx_batch* b)
     int pf = 1, pe = 1;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pf, (const void*)b->B->faces, tmx::kBoundaryThreadsHost, 0);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pe, (const void*)b->B->edges, tmx::kBoundaryThreadsHost, 0);
-    b->grid_faces = b->sms * std::max(1, pf);
-    b->grid_edges = b->sms * std::max(1, pe);
+    pf = std::max(1, pf);
+    pe = std::max(1, pe);
+    b->bound_fit = pf;
+    // persistent boundary grids: bound_bps blocks per SM, or as many as fit
+    b->grid_faces = b->sms * (b->bound_bps > 0 ? std::min(b->bound_bps, pf) : pf);
+    b->grid_edges = b->sms * (b->bound_bps > 0 ? std::min(b->bound_bps, pe) : pe);
     cudaGetLastError();
 }
 
@@ -854,6 +860,25 @@ int tmx_batch_set_sweep(tmx_batch* b, int kind, int zchunk)
     return TMX_OK;
 }
 
+int tmx_batch_set_boundary(tmx_batch* b, int blocks_per_sm)
+{
+    if (!b) return fail(TMX_E_INVALID, "null batch");
+    if (blocks_per_sm < 0) return fail(TMX_E_INVALID, "boundary blocks per SM must be >= 0 (got %d)", blocks_per_sm);
+    TMX_CK(cudaSetDevice(b->device));
+    TMX_CK(cudaStreamSynchronize(b->stream));
+    if (blocks_per_sm != b->bound_bps) drop_graphs(b);
+    b->bound_bps = blocks_per_sm;
+    set_grids(b);
+    return TMX_OK;
+}
+
+int tmx_batch_boundary(const tmx_batch* b, int* blocks_per_sm)
+{
+    if (!b || !blocks_per_sm) return fail(TMX_E_INVALID, "null argument");
+    *blocks_per_sm = b->grid_faces / std::max(1, b->sms);
+    return TMX_OK;
+}
+
 int tmx_batch_shape(const tmx_batch* b, int out[4])
 {
     if (!b || !out) return fail(TMX_E_INVALID, "null argument");
@@ -919,11 +944,27 @@ int tmx_batch_tune(tmx_batch* b, int steps_per_trial, int* threads_out, int* cel
                     bz = kZChunkChoices[zi];
                 }
             }
+    // the boundary kernels' persistent grid with the chosen interior kernel
+    // (they share the SMs with it): 1, 2, 4 blocks per SM or as many as fit
+    int bb = b->bound_bps;
+    if (rc == TMX_OK) rc = tmx_batch_set_shape(b, kBulkThreads[bv], bc);
+    if (rc == TMX_OK && bs) rc = tmx_batch_set_sweep(b, bs, bz);
+    const int bchoices[4] = {1, 2, 4, 0};
+    for (int i = 0; i < 4 && rc == TMX_OK; i++) {
+        if (bchoices[i] >= b->bound_fit) continue;  // the same grid as 0
+        rc = tmx_batch_set_boundary(b, bchoices[i]);
+        if (rc) break;
+        double ms = 0;
+        trial(ms);
+        if (rc == TMX_OK && ms < best) {
+            best = ms;
+            bb = bchoices[i];
+        }
+    }
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
     if (rc) return rc;
-    rc = tmx_batch_set_shape(b, kBulkThreads[bv], bc);
-    if (rc == TMX_OK && bs) rc = tmx_batch_set_sweep(b, bs, bz);
+    rc = tmx_batch_set_boundary(b, bb);
     if (rc) return rc;
     // the trials advanced the mixers: start every one of them again
     TMX_CK(cudaStreamSynchronize(b->stream));
