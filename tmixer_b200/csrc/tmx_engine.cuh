@@ -65,7 +65,7 @@ __device__ __forceinline__ float poly_q_omt(int q, float ux, float uy, float uz,
     return poly_e_omt(EX(q), EY(q), EZ(q), ux, uy, uz, omt);
 }
 
-// Collision of one direction of the interleaved forms with sm_100's packed
+// Collision of one direction of the FP32 form with sm_100's packed
 // two-wide FP32 arithmetic, on the field pairs (flow, A) and (B, C): given
 // the pulled values, the densities, w_q * poly_q (pw) and w_q * rate (wrt),
 // the equilibria f = r * pw and the post-collision values
@@ -73,7 +73,8 @@ __device__ __forceinline__ float poly_q_omt(int q, float ux, float uy, float uz,
 // as in * c1 + c2 * f with c1 = 1 - c2, but rounding one small difference:
 // with c2 = 1/tau near 2, as for tau_c = 0.55, the two large terms of
 // opposite sign cost the species fields several times the FP32 rounding per
-// step.)  c1 is not used.
+// step.)  c1 is not used.  (The FP16-storage form stores o - f, which
+// F16::collide_store forms directly.)
 __device__ __forceinline__ void collide_pairs(float2 in01, float2 in23, float2 r01, float2 r23, float pw, float2,
                                               float2, float2 c2a, float2 c2b, float wrt, float2& o01, float2& o23,
                                               float2& f01, float2& f23)
@@ -227,15 +228,22 @@ struct F32 {
     {
         *(float4*)(Pout + off(0, q, ps, g)) = make_float4(o01.x, o01.y, o23.x, o23.y);
     }
+    // collide direction q of the four fields (collide_pairs) and store it
+    __device__ static void collide_store(S* Pout, int q, long long ps, int g, float2 in01, float2 in23, float2 r01,
+                                         float2 r23, float pw, float2 c1a, float2 c1b, float2 c2a, float2 c2b,
+                                         float wrt)
+    {
+        float2 o01, o23, f01, f23;
+        collide_pairs(in01, in23, r01, r23, pw, c1a, c1b, c2a, c2b, wrt, o01, o23, f01, f23);
+        store_pairs(Pout, q, ps, g, o01, o23, f01, f23);
+    }
     // collide and store the four fields of direction q (packed pairs)
     __device__ static void collide_dir(S* Pout, int q, long long ps, int g, const T (&in)[4], const T (&r)[4], T pw,
                                        const T (&c1)[4], const T (&c2)[4], T w, T rt)
     {
-        float2 o01, o23, f01, f23;
-        collide_pairs(make_float2(in[0], in[1]), make_float2(in[2], in[3]), make_float2(r[0], r[1]),
+        collide_store(Pout, q, ps, g, make_float2(in[0], in[1]), make_float2(in[2], in[3]), make_float2(r[0], r[1]),
                       make_float2(r[2], r[3]), pw, make_float2(c1[0], c1[1]), make_float2(c1[2], c1[3]),
-                      make_float2(c2[0], c2[1]), make_float2(c2[2], c2[3]), w * rt, o01, o23, f01, f23);
-        store_pairs(Pout, q, ps, g, o01, o23, f01, f23);
+                      make_float2(c2[0], c2[1]), make_float2(c2[2], c2[3]), w * rt);
     }
     // fields first .. last-1 (one vector access brings all four)
     __device__ static void decode_fields(const S* __restrict__ Pin, const float4* __restrict__ M, long long ps, int q,
@@ -349,25 +357,32 @@ struct F16 {
         v[2] = b.x;
         v[3] = b.y;
     }
-    __device__ static void store_pairs(S* Pout, int q, long long ps, int g, float2 o01, float2 o23, float2 f01,
-                                       float2 f23)
+    // collide direction q of the four fields and store the stored part of
+    // the result, o - f with f = r * pw the node's own equilibrium, formed
+    // directly: with o = in + c2 * (f - in) - the reaction terms,
+    // o - f = c1 * (in - f) - the reaction terms (c1 = 1 - c2), one FMA on a
+    // difference of the order of the non-equilibrium part, where forming o
+    // first rounds an order-one value and then cancels it
+    __device__ static void collide_store(S* Pout, int q, long long ps, int g, float2 in01, float2 in23, float2 r01,
+                                         float2 r23, float pw, float2 c1a, float2 c1b, float2, float2, float wrt)
     {
-        const __half2 lo = __float22half2_rn(__fadd2_rn(o01, make_float2(-f01.x, -f01.y)));
-        const __half2 hi = __float22half2_rn(__fadd2_rn(o23, make_float2(-f23.x, -f23.y)));
+        const float2 pp = make_float2(pw, pw);
+        const float2 f01 = __fmul2_rn(r01, pp), f23 = __fmul2_rn(r23, pp);
+        const float2 n01 = __ffma2_rn(c1a, __fadd2_rn(in01, make_float2(-f01.x, -f01.y)), make_float2(0.0f, -wrt));
+        const float2 n23 =
+            __ffma2_rn(c1b, __fadd2_rn(in23, make_float2(-f23.x, -f23.y)), make_float2(-wrt, 2.0f * wrt));
+        const __half2 lo = __float22half2_rn(n01), hi = __float22half2_rn(n23);
         uint2 x;
         x.x = *(const unsigned*)&lo;
         x.y = *(const unsigned*)&hi;
         *(uint2*)(Pout + off(0, q, ps, g)) = x;
     }
-    // collide and store the four fields of direction q (packed pairs)
     __device__ static void collide_dir(S* Pout, int q, long long ps, int g, const T (&in)[4], const T (&r)[4], T pw,
                                        const T (&c1)[4], const T (&c2)[4], T w, T rt)
     {
-        float2 o01, o23, f01, f23;
-        collide_pairs(make_float2(in[0], in[1]), make_float2(in[2], in[3]), make_float2(r[0], r[1]),
+        collide_store(Pout, q, ps, g, make_float2(in[0], in[1]), make_float2(in[2], in[3]), make_float2(r[0], r[1]),
                       make_float2(r[2], r[3]), pw, make_float2(c1[0], c1[1]), make_float2(c1[2], c1[3]),
-                      make_float2(c2[0], c2[1]), make_float2(c2[2], c2[3]), w * rt, o01, o23, f01, f23);
-        store_pairs(Pout, q, ps, g, o01, o23, f01, f23);
+                      make_float2(c2[0], c2[1]), make_float2(c2[2], c2[3]), w * rt);
     }
     __device__ static void decode_fields(const S* __restrict__ Pin, const float4* __restrict__ M, long long ps, int q,
                                          int ex, int ey, int ez, T w, int s, T (&v)[4], int first, int last)
@@ -660,11 +675,8 @@ __device__ __forceinline__ void lp_interior(const StepPtrs& X, const Geom& G, co
     const float2 c1a = make_float2((float)P.c1[0], (float)P.c1[1]), c1b = make_float2((float)P.c1[2], (float)P.c1[3]);
     const float2 c2a = make_float2((float)P.c2[0], (float)P.c2[1]), c2b = make_float2((float)P.c2[2], (float)P.c2[3]);
 #pragma unroll
-    for (int q = 0; q < 19; q++) {
-        float2 o01, o23, f01, f23;
-        collide_pairs(p01[q], p23[q], r01, r23, poly[q], c1a, c1b, c2a, c2b, (float)wq(q) * rt, o01, o23, f01, f23);
-        PR::store_pairs(Pout, q, ps, g, o01, o23, f01, f23);
-    }
+    for (int q = 0; q < 19; q++)
+        PR::collide_store(Pout, q, ps, g, p01[q], p23[q], r01, r23, poly[q], c1a, c1b, c2a, c2b, (float)wq(q) * rt);
     if (b == 0 && j == 2 && (i == G.ia || i == G.ib)) {
         T* Rcur = (T*)X.rcur;
         Rcur[g] = rho;
