@@ -6,9 +6,9 @@ index within 1e-3, and the FP64 mass and species totals close.  tau_f is 0.6
 instead of the configuration's 0.52: at 0.52 the reference's own boundary
 closures diverge (the FP64 form, bit-exact with the reference, does too).
 
-Measured (FP32 / FP16 storage): u 1.9e-4 / 1.9e-4, cA and cB 8.9e-5 /
-8.8e-5, cC 3.1e-4 / 3.1e-4, mixing index 2.2e-5 / 2.7e-5, mass 4.9e-6 /
-5.0e-6, species totals up to 1.2e-4 / 6.6e-5.  This case's tau_c = 0.55
+Measured (FP32 / FP16 storage): u 2.0e-4 / 2.0e-4, cA and cB 9.0e-5 /
+8.8e-5, cC 3.2e-4 / 3.1e-4, mixing index 2.2e-5 / 2.8e-5, mass 5.0e-6 /
+5.1e-6, species totals up to 1.2e-4 / 6.5e-5.  This case's tau_c = 0.55
 (relaxation rate 1.82) is where the collision's form matters: written as
 in * (1 - w) + w * feq the species errors were 5 to 15 times larger (cC
 1.35e-3), written as in + w * (feq - in) they are the ones above."""

@@ -610,7 +610,9 @@ int checkpoint_check(const void* buf, long long size, const tmx_case& c, const G
     if (size < (long long)sizeof(CheckpointHeader)) return fail(TMX_E_INVALID, "checkpoint too small");
     CheckpointHeader hd;
     std::memcpy(&hd, buf, sizeof hd);
-    if (std::memcmp(hd.magic, "TMXCKPT1", 8) != 0) return fail(TMX_E_INVALID, "not a checkpoint");
+    if (std::memcmp(hd.magic, "TMXCKPT1", 8) == 0)
+        return fail(TMX_E_INVALID, "checkpoint of an earlier format (FP16 moment records ordered differently)");
+    if (std::memcmp(hd.magic, kCheckpointMagic, 8) != 0) return fail(TMX_E_INVALID, "not a checkpoint");
     if (hd.abi != TMX_ABI_VERSION) return fail(TMX_E_INVALID, "checkpoint of ABI %d, library %d", hd.abi, TMX_ABI_VERSION);
     if (hd.precision != c.precision)
         return fail(TMX_E_INVALID, "checkpoint of precision %d, target %d", hd.precision, c.precision);
@@ -892,7 +894,7 @@ int tmx_checkpoint(tmx_handle* h, void* buf, long long size)
     TMX_CK(cudaSetDevice(h->device));
     TMX_CK(cudaStreamSynchronize(h->stream));
     CheckpointHeader hd{};
-    std::memcpy(hd.magic, "TMXCKPT1", 8);
+    std::memcpy(hd.magic, kCheckpointMagic, 8);
     hd.abi = TMX_ABI_VERSION;
     hd.precision = h->c.precision;
     hd.c = h->c;
@@ -1002,7 +1004,7 @@ int tmx_populations(tmx_handle* h, int box, int fld, double* host_out)
     // the writing node's moments exactly as the kernels do (tmx_engine.cuh)
     std::vector<double> wide(n);
     std::vector<unsigned char> raw(4 * n * h->sbytes);
-    // moment records {(rho, ux, uy, uz), (cA, cB, cC, 1 - 1.5|u|^2)}, 8 floats per node
+    // moment records {(rho, cA, cB, cC), (ux, uy, uz, 1 - 1.5|u|^2)}, 8 floats per node
     std::vector<float> mr(8 * n);
     if (h->K->moments) {
         const float4* m = h->mom[h->cur];
@@ -1023,8 +1025,8 @@ int tmx_populations(tmx_handle* h, int box, int fld, double* host_out)
                 unsigned short hb;
                 std::memcpy(&hb, &raw[e], 2);
                 const float* rec = &mr[8 * t];
-                const float r = fld == 0 ? rec[0] : rec[3 + fld];
-                const float pw = poly_q_host(q, rec[1], rec[2], rec[3], rec[7]) * w;
+                const float r = rec[fld];
+                const float pw = poly_q_host(q, rec[4], rec[5], rec[6], rec[7]) * w;
                 v = std::fmaf(r, pw, half_bits_to_float(hb));
             }
             wide[t] = v;

@@ -637,7 +637,7 @@ int tmx_batch_checkpoint(tmx_batch* b, int slot, void* buf, long long bytes)
     TMX_CK(cudaSetDevice(b->device));
     TMX_CK(cudaStreamSynchronize(b->stream));
     CheckpointHeader hd{};
-    std::memcpy(hd.magic, "TMXCKPT1", 8);
+    std::memcpy(hd.magic, kCheckpointMagic, 8);
     hd.abi = TMX_ABI_VERSION;
     hd.precision = b->precision;
     hd.c = s.c;

@@ -261,10 +261,12 @@ struct F32 {
 
 // FP32 arithmetic; populations stored in FP16 as their non-equilibrium part
 // n_q = f_q - feq_q(rho, u) of the node that wrote them, next to that node's
-// FP32 moments M = {(rho, ux, uy, uz), (cA, cB, cC, 1 - 1.5|u|^2)}, one 32-byte
-// record per node (float4 M[2g], M[2g+1]).  A
-// reader adds back feq_q of the writer's moments.  The stored quantity is of
-// the order of the gradients, so FP16 keeps about FP32 accuracy of f.
+// FP32 moments M = {(rho, cA, cB, cC), (ux, uy, uz, 1 - 1.5|u|^2)}, one 32-byte
+// record per node (float4 M[2g], M[2g+1]; the densities in field-pair order,
+// so that a pair (rho, cA) or (cB, cC) is one register pair of the packed
+// arithmetic).  A reader adds back feq_q of the writer's moments.  The stored
+// quantity is of the order of the gradients, so FP16 keeps about FP32
+// accuracy of f.
 struct F16 {
     using T = float;
     using S = __half;
@@ -307,10 +309,10 @@ struct F16 {
     }
     __device__ static bool tiny(T) { return false; }
     __device__ static T feq(T r, T pw, int, bool) { return __fmul_rn(r, pw); }
-    // w_q * poly_q of a writer from its moment record {(rho, u), (c, omt)}
+    // w_q * poly_q of a writer from its moment record {(rho, c), (u, omt)}
     __device__ static T src_pw(int q, const float4& mf, const float4& ms)
     {
-        return __fmul_rn(poly_q_omt(q, mf.y, mf.z, mf.w, ms.w), (float)wq(q));
+        return __fmul_rn(poly_q_omt(q, ms.x, ms.y, ms.z, ms.w), (float)wq(q));
     }
     __device__ static T pw_dir(int ex, int ey, int ez, T w, T ux, T uy, T uz)
     {
@@ -342,10 +344,10 @@ struct F16 {
                                       float2& v01, float2& v23)
     {
         const float2 raw01 = __half22float2(*(const __half2*)&x.x), raw23 = __half22float2(*(const __half2*)&x.y);
-        const float pw = __fmul_rn(poly_e_omt(ex, ey, ez, mf.y, mf.z, mf.w, ms.w), w);
+        const float pw = __fmul_rn(poly_e_omt(ex, ey, ez, ms.x, ms.y, ms.z, ms.w), w);
         const float2 pp = make_float2(pw, pw);
-        v01 = __ffma2_rn(make_float2(mf.x, ms.x), pp, raw01);
-        v23 = __ffma2_rn(make_float2(ms.y, ms.z), pp, raw23);
+        v01 = __ffma2_rn(make_float2(mf.x, mf.y), pp, raw01);
+        v23 = __ffma2_rn(make_float2(mf.z, mf.w), pp, raw23);
     }
     __device__ static void decode4(const S* __restrict__ Pin, const float4* __restrict__ M, long long ps, int q,
                                    int ex, int ey, int ez, T w, int s, T (&v)[4])
@@ -396,7 +398,7 @@ struct F16 {
     __device__ static T decode(const S* p, int fld, int q, const float4* M, long long, int src)
     {
         const float4 mf = __ldg(M + 2 * (long long)src), ms = __ldg(M + 2 * (long long)src + 1);
-        const float r = fld == 0 ? mf.x : (fld == 1 ? ms.x : (fld == 2 ? ms.y : ms.z));
+        const float r = fld == 0 ? mf.x : (fld == 1 ? mf.y : (fld == 2 ? mf.z : mf.w));
         return __half2float(__ldg(p)) + feq(r, src_pw(q, mf, ms), q, false);
     }
     __device__ static void encode(S* p, T v, T feq) { *p = __float2half_rn(v - feq); }
@@ -484,8 +486,8 @@ __device__ __forceinline__ void init_node(const StepPtrs& X, const Geom& G, cons
 #pragma unroll
     for (int m = 1; m < 7; m++) Mac[m * ps + g] = 0.0;
     if (PR::kMoments) {
-        X.mcur[2 * (long long)g] = make_float4((float)rho0, 0.f, 0.f, 0.f);
-        X.mcur[2 * (long long)g + 1] = make_float4(0.f, 0.f, 0.f, omt_term(0.f, 0.f, 0.f));
+        X.mcur[2 * (long long)g] = make_float4((float)rho0, 0.f, 0.f, 0.f);  // rho0, no species
+        X.mcur[2 * (long long)g + 1] = make_float4(0.f, 0.f, 0.f, omt_term(0.f, 0.f, 0.f));  // at rest
     }
 }
 
@@ -579,9 +581,9 @@ __device__ __forceinline__ void bulk_node(const StepPtrs& X, const Geom& G, cons
         Rcur[3 * ps + g] = cc;
     }
     if (PR::kMoments) {
-        X.mcur[2 * (long long)g] = make_float4((float)rho, (float)ux, (float)uy, (float)uz);
+        X.mcur[2 * (long long)g] = make_float4((float)rho, (float)ca, (float)cb, (float)cc);
         X.mcur[2 * (long long)g + 1] =
-            make_float4((float)ca, (float)cb, (float)cc, omt_term((float)ux, (float)uy, (float)uz));
+            make_float4((float)ux, (float)uy, (float)uz, omt_term((float)ux, (float)uy, (float)uz));
     }
     if (write_macro) {
         double* Mac = X.mac;
@@ -685,9 +687,9 @@ __device__ __forceinline__ void lp_interior(const StepPtrs& X, const Geom& G, co
         Rcur[3 * ps + g] = cc;
     }
     if (PR::kMoments) {
-        X.mcur[2 * (long long)g] = make_float4((float)rho, (float)ux, (float)uy, (float)uz);
+        X.mcur[2 * (long long)g] = make_float4((float)rho, (float)ca, (float)cb, (float)cc);
         X.mcur[2 * (long long)g + 1] =
-            make_float4((float)ca, (float)cb, (float)cc, omt_term((float)ux, (float)uy, (float)uz));
+            make_float4((float)ux, (float)uy, (float)uz, omt_term((float)ux, (float)uy, (float)uz));
     }
     if (write_macro) {
         double* Mac = X.mac;
@@ -774,9 +776,9 @@ __device__ __forceinline__ void zwall_node(const StepPtrs& X, const Geom& G, con
     Rcur[2 * ps + gw] = cb;
     Rcur[3 * ps + gw] = ccc;
     if constexpr (PR::kMoments) {
-        X.mcur[2 * (long long)gw] = make_float4((float)rho, (float)ux, (float)uy, (float)uz);
+        X.mcur[2 * (long long)gw] = make_float4((float)rho, (float)ca, (float)cb, (float)ccc);
         X.mcur[2 * (long long)gw + 1] =
-            make_float4((float)ca, (float)cb, (float)ccc, omt_term((float)ux, (float)uy, (float)uz));
+            make_float4((float)ux, (float)uy, (float)uz, omt_term((float)ux, (float)uy, (float)uz));
     }
     if (write_macro) {
         double* Mac = X.mac;
@@ -1499,10 +1501,10 @@ __device__ __forceinline__ void boundary_lane(const StepPtrs& X, const Geom& G, 
 
     Rcur[fld * ps + c.g] = r;
     if (PR::kMoments) {
-        if (fld == 0) X.mcur[2 * (long long)c.g] = make_float4((float)rho, (float)ux, (float)uy, (float)uz);
+        if (fld == 0) X.mcur[2 * (long long)c.g] = make_float4((float)rho, (float)ca, (float)cb, (float)cc);
         if (fld == 1)
             X.mcur[2 * (long long)c.g + 1] =
-                make_float4((float)ca, (float)cb, (float)cc, omt_term((float)ux, (float)uy, (float)uz));
+                make_float4((float)ux, (float)uy, (float)uz, omt_term((float)ux, (float)uy, (float)uz));
     }
     if (write_macro) {
         Mac[(fld == 0 ? 0 : 3 + fld) * ps + c.g] = r;
@@ -1655,10 +1657,10 @@ __device__ __forceinline__ void boundary_lane_lp(const StepPtrs& X, const Geom& 
 
     Rcur[fld * ps + c.g] = r;
     if (PR::kMoments) {
-        if (fld == 0) X.mcur[2 * (long long)c.g] = make_float4((float)rho, (float)ux, (float)uy, (float)uz);
+        if (fld == 0) X.mcur[2 * (long long)c.g] = make_float4((float)rho, (float)ca, (float)cb, (float)cc);
         if (fld == 1)
             X.mcur[2 * (long long)c.g + 1] =
-                make_float4((float)ca, (float)cb, (float)cc, omt_term((float)ux, (float)uy, (float)uz));
+                make_float4((float)ux, (float)uy, (float)uz, omt_term((float)ux, (float)uy, (float)uz));
     }
     if (write_macro) {
         Mac[(fld == 0 ? 0 : 3 + fld) * ps + c.g] = r;

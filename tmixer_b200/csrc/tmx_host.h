@@ -138,8 +138,11 @@ inline void sweep_tiles(const Geom& G, int mixer, int ty, int zchunk, std::vecto
 // densities (4 planes, arithmetic type), the FP16 form's moment records
 // (2 float4 per node, or nothing), the macroscopic fields (7 FP64 planes) and
 // the two inlet profiles ((iny+3)(nz+3) FP64 values each).
+// "TMXCKPT2": FP16 records {(rho, cA, cB, cC), (ux, uy, uz, omt)};
+// "TMXCKPT1" (refused) had {(rho, ux, uy, uz), (cA, cB, cC, omt)}
+constexpr char kCheckpointMagic[9] = "TMXCKPT2";
 struct CheckpointHeader {
-    char magic[8];  // "TMXCKPT1"
+    char magic[8];  // kCheckpointMagic
     int abi;
     int precision;
     tmx_case c;
