@@ -90,6 +90,15 @@ def case_nodes(p: dict) -> int:
     return p["inx"] * p["iny"] * p["nz"] + p["mnx"] * p["mny"] * p["nz"]
 
 
+def interior_nodes(s) -> int:
+    """Interior (non-boundary) nodes of a case: the inlet box's inner nodes
+    plus its row y = 1 over the opening (mnx - 2 columns), and the mixing
+    box's inner columns over rows 2..mny (row mny joins the inlet box)."""
+    inlet = (s.nz - 2) * ((s.inx - 2) * (s.iny - 2) + (s.mnx - 2))
+    mixing = (s.mnx - 2) * (s.mny - 1) * (s.nz - 2)
+    return inlet + mixing
+
+
 def w_layout_umean(W: int, u_max: float) -> float:
     """The reference's Umean for a W-layout mixer whose duct profile peaks at
     u_max, computed without the CUDA library (the reference arm must not load
@@ -518,9 +527,16 @@ def run_batched(args, dist: Dist, fp64_mlups: float, peaks: dict) -> dict:
         B.step(args.warmup, write_macro=False)
         B.sync()
         ms = B.time_steps(args.batched_steps)
+        # each kernel alone (the interior kernel after the boundary kernels)
+        kt = min(args.batched_steps, 50)
+        t_int, t_bnd, _ = B.step_timed(kt)
         B.step(1, write_macro=True)
         im = B.outlet_im()
         B_shape = B.shape()
+    # nodes the interior kernel updates: the interior ones, and with a sweep
+    # shape the z wall faces (one at each end of every interior column)
+    swept = B_shape["kernel"] != "flat"
+    upd = sum(interior_nodes(s) * (s.nz / (s.nz - 2) if swept else 1) for s in specs)
     mlups = nodes * args.batched_steps / (ms * 1e-3) / 1e6
     bpl = FORM_BYTES["fp16"]
     gbs = mlups * 1e6 * bpl / 1e9
@@ -528,7 +544,13 @@ def run_batched(args, dist: Dist, fp64_mlups: float, peaks: dict) -> dict:
             "vs_plain_fp64": mlups / fp64_mlups if fp64_mlups else None,
             "roofline": {"bound": "hbm", "achieved": gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": gbs / peaks["hbm_gbs"], "algorithmic_bytes_per_lup": bpl,
-                         "frac_populations_only": mlups * 1e6 * 304 / 1e9 / peaks["hbm_gbs"]},
+                         "frac_populations_only": mlups * 1e6 * 304 / 1e9 / peaks["hbm_gbs"],
+                         "interior_kernel": {
+                             "what": "the interior kernel alone (%d timed steps, boundary kernels before it), "
+                                     "%d nodes per launch x %d B" % (kt, int(upd), bpl),
+                             "ms": t_int / kt, "achieved": upd * bpl / (t_int / kt * 1e-3) / 1e9,
+                             "frac": upd * bpl / (t_int / kt * 1e-3) / 1e9 / peaks["hbm_gbs"]},
+                         "boundary_kernels_ms": t_bnd / kt},
             "tuned": tuned, "launch_shape": B_shape,
             "nonfinite_outlet_im": int(sum(1 for r in im for v in r if v != v)),
             "config": "%d mixers, W from %s, u_max U[0.02,0.08], tau_f U%s (configuration U%s), tau_c U[0.52,0.7], "

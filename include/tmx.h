@@ -230,8 +230,11 @@ int tmx_inlet_profile(tmx_handle *h, double *uin1, double *uin2);
 
 /* Run nsteps steps with CUDA events around every kernel launch on the
  * handle's stream and return the summed device times (ms) of the bulk
- * (interior) kernel, of the boundary kernel and of the whole step loop.
- * Benchmark support; no counterpart in the reference. */
+ * (interior) kernel, of the boundary kernels and of the whole step loop.
+ * The interior kernel runs after the boundary kernels here in every form
+ * (tmx_step overlaps them in the FP32 and FP16 forms), so that each time is
+ * that of its kernels alone.  Benchmark support; no counterpart in the
+ * reference. */
 int tmx_step_timed(tmx_handle *h, int nsteps, double *ms_bulk, double *ms_boundary, double *ms_total);
 
 /* Run nsteps steps exactly as tmx_step does, between two CUDA events recorded
@@ -362,6 +365,13 @@ int tmx_batch_shape(const tmx_batch *b, int out[4]);
 
 /* Run nsteps steps between two CUDA events on the batch's stream and return
  * the elapsed device time (ms). */
+
+/* Run nsteps steps (without the captured graphs) with CUDA events around the
+ * interior kernel and around the boundary kernels, the interior kernel after
+ * the boundary kernels in every form so that each time is that of its
+ * kernels alone, and return the summed device times (ms) and that of the
+ * whole loop.  Benchmark support; no counterpart in the reference. */
+int tmx_batch_step_timed(tmx_batch *b, int nsteps, double *ms_interior, double *ms_boundary, double *ms_total);
 int tmx_batch_time_steps(tmx_batch *b, int nsteps, double *ms);
 
 /* Free the batch, its arena and its mixers. */

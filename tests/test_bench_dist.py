@@ -60,6 +60,9 @@ def test_workload_spec_geometry():
     spec = bench.workload_spec()
     assert spec.nodes() == 524288 and (spec.inx, spec.mnx, spec.mny) == (256, 64, 128)
     assert spec.tau == bench.WORKLOAD["tau_f"]
+    # interior nodes of the W=32 mixer (the library's count: 524,288 fluid
+    # nodes less 57,608 boundary nodes)
+    assert bench.interior_nodes(spec) == 466680
 
 
 def test_measured_peaks_present_or_fallback():

@@ -125,6 +125,22 @@ def test_boundary_grids_agree(gpu, precision, bps):
         assert B.shape()["boundary_blocks_per_sm"] > bps
 
 
+def test_step_timed_agrees(gpu):
+    """Timed steps (kernels one after another, no graph) give each mixer its
+    solo run's bits and count as steps."""
+    specs = _specs(T.TMX_FP16)
+    with T.Batch(T.TMX_FP16, budget=1 << 28) as B:
+        B.set_sweep(T.SHAPE_SWEEP4, 4)
+        slots = [B.add(s) for s in specs]
+        B.step(3)
+        ti, tb, tt = B.step_timed(4)
+        assert ti > 0 and tb > 0 and tt >= ti
+        B.step(1)
+        for slot, spec in zip(slots, specs):
+            assert B.slot_steps(slot) == 8
+            _same(B, slot, _alone(spec, 8), 8)
+
+
 @pytest.mark.parametrize("threads,cells", [(128, 1024), (512, 8192)])
 def test_launch_shapes_agree(gpu, threads, cells):
     specs = _specs(T.TMX_FP32)

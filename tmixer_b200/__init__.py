@@ -148,6 +148,7 @@ def lib() -> ctypes.CDLL:
     L.tmx_batch_set_sweep.argtypes = [vp, ip, ip]
     L.tmx_batch_shape.argtypes = [vp, P(ip)]
     L.tmx_batch_set_boundary.argtypes = [vp, ip]
+    L.tmx_batch_step_timed.argtypes = [vp, ip, P(dp), P(dp), P(dp)]
     L.tmx_batch_boundary.argtypes = [vp, P(ip)]
     L.tmx_batch_checkpoint_size.argtypes = [vp, ip, P(LL)]
     L.tmx_batch_checkpoint.argtypes = [vp, ip, vp, LL]
@@ -541,6 +542,13 @@ class Batch:
         ms = ctypes.c_double()
         _check(lib().tmx_batch_time_steps(self._b, int(n), ctypes.byref(ms)))
         return ms.value
+
+    def step_timed(self, n: int):
+        """(interior ms, boundary ms, total ms) of n steps with each kernel
+        timed alone (tmx_batch_step_timed)."""
+        a, b, t = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        _check(lib().tmx_batch_step_timed(self._b, int(n), ctypes.byref(a), ctypes.byref(b), ctypes.byref(t)))
+        return a.value, b.value, t.value
 
     def close(self) -> None:
         if self._b:

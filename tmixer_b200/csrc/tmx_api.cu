@@ -507,7 +507,9 @@ int enqueue_step(tmx_handle* h, int cur, int write_macro, cudaEvent_t* ev)
     // 202 us in order at W=32).  The reduced-precision boundary kernels (64
     // registers) do overlap the bulk kernel (FP16 step 75 us side by side,
     // 85 us in order).
-    if (h->K->serial) {
+    // (timed steps, ev given, run the interior kernel after the boundary
+    // kernels in every form, so that each event pair times its kernels alone)
+    if (h->K->serial || ev) {
         TMX_CK(cudaStreamWaitEvent(h->stream, h->join, 0));
         TMX_CK(cudaStreamWaitEvent(h->stream, h->join2, 0));
     }
@@ -518,7 +520,7 @@ int enqueue_step(tmx_handle* h, int cur, int write_macro, cudaEvent_t* ev)
     else
         h->K->bulk<<<h->bulk_blocks, 256, 0, h->stream>>>(X, G, h->P, write_macro);
     if (ev) TMX_CK(cudaEventRecord(ev[1], h->stream));
-    if (!h->K->serial) {
+    if (!h->K->serial && !ev) {
         TMX_CK(cudaStreamWaitEvent(h->stream, h->join, 0));
         TMX_CK(cudaStreamWaitEvent(h->stream, h->join2, 0));
     }

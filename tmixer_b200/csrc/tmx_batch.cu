@@ -351,22 +351,32 @@ int rebuild(tmx_batch* b)
     return TMX_OK;
 }
 
-int enqueue(tmx_batch* b, int parity, int write_macro)
+// One batch step on the batch's streams.  With ev (4 events: interior start
+// and end, boundary start and end) the interior kernel runs after the
+// boundary kernels in every form, so that each event pair times its kernels
+// alone (tmx_batch_step_timed).
+int enqueue(tmx_batch* b, int parity, int write_macro, cudaEvent_t* ev = nullptr)
 {
     TMX_CK(cudaEventRecord(b->fork, b->stream));
     TMX_CK(cudaStreamWaitEvent(b->aux, b->fork, 0));
     TMX_CK(cudaStreamWaitEvent(b->aux2, b->fork, 0));
+    if (ev) TMX_CK(cudaEventRecord(ev[2], b->aux));
     const int bt = tmx::kBoundaryThreadsHost;
     b->B->faces<<<b->grid_faces, bt, 0, b->aux>>>(b->d_desc, b->d_faces, b->d_counts, parity, write_macro);
     b->B->edges<<<b->grid_edges, bt, 0, b->aux2>>>(b->d_desc, b->d_edges, b->d_counts, parity, write_macro);
     TMX_CK(cudaEventRecord(b->join2, b->aux2));
+    if (ev) {
+        TMX_CK(cudaStreamWaitEvent(b->aux, b->join2, 0));
+        TMX_CK(cudaEventRecord(ev[3], b->aux));
+    }
     TMX_CK(cudaEventRecord(b->join, b->aux));
     // in order for FP64, side by side for the reduced-precision forms (as the
     // single-mixer step; StepKernels::serial)
-    if (b->K->serial) {
+    if (b->K->serial || ev) {
         TMX_CK(cudaStreamWaitEvent(b->stream, b->join, 0));
         TMX_CK(cudaStreamWaitEvent(b->stream, b->join2, 0));
     }
+    if (ev) TMX_CK(cudaEventRecord(ev[0], b->stream));
     if (const SweepShape* sh = b->sweep ? sweep_shape(b->sweep) : nullptr)
         sh->batch<<<b->grid_sweep[b->sweep], sh->threads(), sh->smem(), b->stream>>>(b->d_desc, b->d_tiles,
                                                                                     b->d_counts, parity, write_macro);
@@ -374,7 +384,8 @@ int enqueue(tmx_batch* b, int parity, int write_macro)
         b->B->bulk[b->variant]<<<b->grid_bulk[b->variant], kBulkThreads[b->variant], 0, b->stream>>>(
             b->d_desc, b->d_blocks, b->d_counts, parity, write_macro);
     TMX_CK(cudaGetLastError());
-    if (!b->K->serial) {
+    if (ev) TMX_CK(cudaEventRecord(ev[1], b->stream));
+    if (!b->K->serial && !ev) {
         TMX_CK(cudaStreamWaitEvent(b->stream, b->join, 0));
         TMX_CK(cudaStreamWaitEvent(b->stream, b->join2, 0));
     }
@@ -978,6 +989,59 @@ int tmx_batch_tune(tmx_batch* b, int steps_per_trial, int* threads_out, int* cel
     if (threads_out) *threads_out = bs ? sweep_shape(bs)->threads() : kBulkThreads[bv];
     if (cells_out) *cells_out = bs ? sweep_shape(bs)->threads() * bz : bc;
     if (ms_out) *ms_out = best;
+    return TMX_OK;
+}
+
+int tmx_batch_step_timed(tmx_batch* b, int nsteps, double* ms_interior, double* ms_boundary, double* ms_total)
+{
+    if (!b) return fail(TMX_E_INVALID, "null batch");
+    if (nsteps <= 0) return fail(TMX_E_INVALID, "nsteps must be positive");
+    TMX_CK(cudaSetDevice(b->device));
+    if (b->dirty) {
+        int rc = rebuild(b);
+        if (rc) return rc;
+    }
+    std::vector<cudaEvent_t> ev((size_t)nsteps * 4, nullptr);
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    cudaError_t e = cudaSuccess;
+    for (auto& x : ev)
+        if (e == cudaSuccess) e = cudaEventCreate(&x);
+    if (e == cudaSuccess) e = cudaEventCreate(&t0);
+    if (e == cudaSuccess) e = cudaEventCreate(&t1);
+    int rc = e == cudaSuccess ? TMX_OK : fail(TMX_E_CUDA, "tmx_batch_step_timed: %s", cudaGetErrorString(e));
+    if (rc == TMX_OK && cudaEventRecord(t0, b->stream) != cudaSuccess) rc = fail(TMX_E_CUDA, "event record failed");
+    int done = 0;
+    for (; done < nsteps && rc == TMX_OK; done++) {
+        rc = enqueue(b, b->parity, 0, &ev[(size_t)done * 4]);
+        if (rc == TMX_OK) {
+            b->parity ^= 1;
+            b->steps++;
+        }
+    }
+    for (auto& s : b->slots)
+        if (s.used) s.steps += done - (rc == TMX_OK ? 0 : 1);
+    double si = 0, sb = 0;
+    float tot = 0;
+    if (rc == TMX_OK) {
+        cudaEventRecord(t1, b->stream);
+        if (cudaEventSynchronize(t1) != cudaSuccess) rc = fail(TMX_E_CUDA, "tmx_batch_step_timed: event wait failed");
+    }
+    for (int s = 0; s < nsteps && rc == TMX_OK; s++) {
+        float a = 0, c = 0;
+        cudaEventElapsedTime(&a, ev[(size_t)s * 4], ev[(size_t)s * 4 + 1]);
+        cudaEventElapsedTime(&c, ev[(size_t)s * 4 + 2], ev[(size_t)s * 4 + 3]);
+        si += a;
+        sb += c;
+    }
+    if (rc == TMX_OK) cudaEventElapsedTime(&tot, t0, t1);
+    for (auto& x : ev)
+        if (x) cudaEventDestroy(x);
+    if (t0) cudaEventDestroy(t0);
+    if (t1) cudaEventDestroy(t1);
+    if (rc) return rc;
+    if (ms_interior) *ms_interior = si;
+    if (ms_boundary) *ms_boundary = sb;
+    if (ms_total) *ms_total = tot;
     return TMX_OK;
 }
 
