@@ -339,7 +339,8 @@ int tmx_batch_set_shape(tmx_batch *b, int threads, int cells);
  * kernel's (threads, cells) choices; for the FP16 form also every sweep
  * shape with 4, 8, 16 or 32 planes per tile, i.e. nodes per thread), keep
  * the fastest, then with it the boundary kernels' grid (1, 2 or 4 blocks per
- * SM or as many as fit, tmx_batch_set_boundary), keep the fastest, then
+ * SM or as many as fit) and order (beside the interior kernel or before it,
+ * tmx_batch_set_boundary), keep the fastest, then
  * start every mixer again from its initial state.  Returns the threads per
  * block, the nodes per cell block (flat) or per tile (sweep), and the time
  * per step (ms); tmx_batch_shape and tmx_batch_boundary tell what won. */
@@ -353,10 +354,12 @@ int tmx_batch_set_sweep(tmx_batch *b, int kind, int zchunk);
 
 /* The boundary (face and edge) kernels' persistent grid: blocks_per_sm
  * blocks of 128 threads per SM, at most as many as fit; 0 (the default): as
- * many as fit.  tmx_batch_boundary returns the face kernel's blocks per SM
- * in use.  No counterpart in the reference. */
-int tmx_batch_set_boundary(tmx_batch *b, int blocks_per_sm);
-int tmx_batch_boundary(const tmx_batch *b, int *blocks_per_sm);
+ * many as fit.  after = 1 runs the interior kernel after them, 0 (the
+ * default) beside them; the FP64 form always runs it after them.
+ * tmx_batch_boundary returns the face kernel's blocks per SM in use and the
+ * order (after may be NULL).  No counterpart in the reference. */
+int tmx_batch_set_boundary(tmx_batch *b, int blocks_per_sm, int after);
+int tmx_batch_boundary(const tmx_batch *b, int *blocks_per_sm, int *after);
 
 /* The interior kernel's shape: out[0] TMX_SHAPE_*,
  * out[1] threads per block, out[2] nodes per cell block of the flat kernel,

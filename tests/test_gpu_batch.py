@@ -101,28 +101,33 @@ def test_tune_restarts_mixers(gpu):
         assert best["kernel"] in T.SHAPE_NAMES.values()
         assert best["threads"] in (128, 256, 512) and best["cells"] % best["threads"] == 0
         shape = B.shape()
-        assert all(shape[k] == best[k] for k in ("kernel", "threads", "cells", "zchunk", "boundary_blocks_per_sm"))
+        assert all(shape[k] == best[k] for k in ("kernel", "threads", "cells", "zchunk", "boundary_blocks_per_sm",
+                                                 "interior_after_boundary"))
         assert shape["boundary_blocks_per_sm"] >= 1
         B.step(11)
         for slot, spec in zip(slots, specs):
             _same(B, slot, _alone(spec, 11), 11)
 
 
-@pytest.mark.parametrize("precision,bps", [(T.TMX_FP16, 1), (T.TMX_FP64, 2)])
-def test_boundary_grids_agree(gpu, precision, bps):
+@pytest.mark.parametrize("precision,bps,after", [(T.TMX_FP16, 1, False), (T.TMX_FP16, 0, True),
+                                                 (T.TMX_FP64, 2, False)])
+def test_boundary_grids_agree(gpu, precision, bps, after):
     """A smaller persistent grid of the boundary kernels (each block then
     takes more 32-entry chunks, of several mixers) gives each mixer its solo
     run's bits."""
     specs = _specs(precision)
     with T.Batch(precision, budget=1 << 28) as B:
-        B.set_boundary(bps)
-        assert B.shape()["boundary_blocks_per_sm"] == bps
+        B.set_boundary(bps, after)
+        shape = B.shape()
+        assert shape["interior_after_boundary"] == (after or precision == T.TMX_FP64)
+        if bps:
+            assert shape["boundary_blocks_per_sm"] == bps
         slots = [B.add(s) for s in specs]
         B.step(6)
         for slot, spec in zip(slots, specs):
             _same(B, slot, _alone(spec, 6), 6)
         B.set_boundary(0)
-        assert B.shape()["boundary_blocks_per_sm"] > bps
+        assert B.shape()["boundary_blocks_per_sm"] > max(bps, 1)
 
 
 def test_step_timed_agrees(gpu):

@@ -147,9 +147,9 @@ def lib() -> ctypes.CDLL:
     L.tmx_batch_time_steps.argtypes = [vp, ip, P(dp)]
     L.tmx_batch_set_sweep.argtypes = [vp, ip, ip]
     L.tmx_batch_shape.argtypes = [vp, P(ip)]
-    L.tmx_batch_set_boundary.argtypes = [vp, ip]
+    L.tmx_batch_set_boundary.argtypes = [vp, ip, ip]
     L.tmx_batch_step_timed.argtypes = [vp, ip, P(dp), P(dp), P(dp)]
-    L.tmx_batch_boundary.argtypes = [vp, P(ip)]
+    L.tmx_batch_boundary.argtypes = [vp, P(ip), P(ip)]
     L.tmx_batch_checkpoint_size.argtypes = [vp, ip, P(LL)]
     L.tmx_batch_checkpoint.argtypes = [vp, ip, vp, LL]
     L.tmx_batch_restore.argtypes = [vp, P(_CCase), vp, LL, P(ip)]
@@ -507,19 +507,20 @@ class Batch:
         with zchunk planes per tile."""
         _check(lib().tmx_batch_set_sweep(self._b, int(kind), int(zchunk)))
 
-    def set_boundary(self, blocks_per_sm: int) -> None:
+    def set_boundary(self, blocks_per_sm: int, after: bool = False) -> None:
         """The boundary kernels' persistent grid in blocks per SM (0: as many
-        as fit)."""
-        _check(lib().tmx_batch_set_boundary(self._b, int(blocks_per_sm)))
+        as fit), and whether the interior kernel runs after them (else beside
+        them; the FP64 form always after)."""
+        _check(lib().tmx_batch_set_boundary(self._b, int(blocks_per_sm), 1 if after else 0))
 
     def shape(self) -> dict:
         o = (ctypes.c_int * 4)()
         _check(lib().tmx_batch_shape(self._b, o))
-        bb = ctypes.c_int()
-        _check(lib().tmx_batch_boundary(self._b, ctypes.byref(bb)))
+        bb, ba = ctypes.c_int(), ctypes.c_int()
+        _check(lib().tmx_batch_boundary(self._b, ctypes.byref(bb), ctypes.byref(ba)))
         return dict(kernel=SHAPE_NAMES[o[0]], threads=o[1], cells=o[2], zchunk=o[3],
                     nodes_per_thread=(o[2] // o[1]) if o[0] == SHAPE_FLAT else o[3],
-                    boundary_blocks_per_sm=bb.value)
+                    boundary_blocks_per_sm=bb.value, interior_after_boundary=bool(ba.value))
 
     def set_from(self, shape: dict) -> None:
         """Apply a shape() dictionary (e.g. the tuned shape of another batch)."""
@@ -528,7 +529,7 @@ class Batch:
         else:
             self.set_sweep(SHAPE_KINDS[shape["kernel"]], shape["zchunk"])
         if "boundary_blocks_per_sm" in shape:
-            self.set_boundary(shape["boundary_blocks_per_sm"])
+            self.set_boundary(shape["boundary_blocks_per_sm"], shape.get("interior_after_boundary", False))
 
     def tune(self, steps_per_trial: int = 20) -> dict:
         """Autotune the interior kernel's shape (tmx_batch_tune) and return it

@@ -221,6 +221,7 @@ struct tmx_batch {
     int sweep = 0;       // 0: the flat kernel; else the TMX_SHAPE_SWEEP* shape of the interior
     int zchunk = 8;      // planes per sweep tile
     int bound_bps = 0;   // boundary kernels' blocks per SM (0: as many as fit)
+    int bound_after = 0; // reduced-precision forms: interior kernel after the boundary kernels (1) or beside them
     int bound_fit = 1;   // blocks of the face kernel that fit on an SM
     int sms = 148;
     int grid_bulk[3] = {0, 0, 0};
@@ -372,7 +373,7 @@ int enqueue(tmx_batch* b, int parity, int write_macro, cudaEvent_t* ev = nullptr
     TMX_CK(cudaEventRecord(b->join, b->aux));
     // in order for FP64, side by side for the reduced-precision forms (as the
     // single-mixer step; StepKernels::serial)
-    if (b->K->serial || ev) {
+    if (b->K->serial || b->bound_after || ev) {
         TMX_CK(cudaStreamWaitEvent(b->stream, b->join, 0));
         TMX_CK(cudaStreamWaitEvent(b->stream, b->join2, 0));
     }
@@ -385,7 +386,7 @@ int enqueue(tmx_batch* b, int parity, int write_macro, cudaEvent_t* ev = nullptr
             b->d_desc, b->d_blocks, b->d_counts, parity, write_macro);
     TMX_CK(cudaGetLastError());
     if (ev) TMX_CK(cudaEventRecord(ev[1], b->stream));
-    if (!b->K->serial && !ev) {
+    if (!b->K->serial && !b->bound_after && !ev) {
         TMX_CK(cudaStreamWaitEvent(b->stream, b->join, 0));
         TMX_CK(cudaStreamWaitEvent(b->stream, b->join2, 0));
     }
@@ -871,22 +872,25 @@ int tmx_batch_set_sweep(tmx_batch* b, int kind, int zchunk)
     return TMX_OK;
 }
 
-int tmx_batch_set_boundary(tmx_batch* b, int blocks_per_sm)
+int tmx_batch_set_boundary(tmx_batch* b, int blocks_per_sm, int after)
 {
     if (!b) return fail(TMX_E_INVALID, "null batch");
     if (blocks_per_sm < 0) return fail(TMX_E_INVALID, "boundary blocks per SM must be >= 0 (got %d)", blocks_per_sm);
+    if (after != 0 && after != 1) return fail(TMX_E_INVALID, "after must be 0 or 1 (got %d)", after);
     TMX_CK(cudaSetDevice(b->device));
     TMX_CK(cudaStreamSynchronize(b->stream));
-    if (blocks_per_sm != b->bound_bps) drop_graphs(b);
+    if (blocks_per_sm != b->bound_bps || after != b->bound_after) drop_graphs(b);
     b->bound_bps = blocks_per_sm;
+    b->bound_after = after;
     set_grids(b);
     return TMX_OK;
 }
 
-int tmx_batch_boundary(const tmx_batch* b, int* blocks_per_sm)
+int tmx_batch_boundary(const tmx_batch* b, int* blocks_per_sm, int* after)
 {
     if (!b || !blocks_per_sm) return fail(TMX_E_INVALID, "null argument");
     *blocks_per_sm = b->grid_faces / std::max(1, b->sms);
+    if (after) *after = (b->K->serial || b->bound_after) ? 1 : 0;
     return TMX_OK;
 }
 
@@ -955,27 +959,30 @@ int tmx_batch_tune(tmx_batch* b, int steps_per_trial, int* threads_out, int* cel
                     bz = kZChunkChoices[zi];
                 }
             }
-    // the boundary kernels' persistent grid with the chosen interior kernel
-    // (they share the SMs with it): 1, 2, 4 blocks per SM or as many as fit
-    int bb = b->bound_bps;
+    // the boundary kernels with the chosen interior kernel (they share the
+    // SMs with it): a persistent grid of 1, 2, 4 blocks per SM or as many as
+    // fit, beside the interior kernel or (reduced-precision forms) before it
+    int bb = b->bound_bps, ba = b->bound_after;
     if (rc == TMX_OK) rc = tmx_batch_set_shape(b, kBulkThreads[bv], bc);
     if (rc == TMX_OK && bs) rc = tmx_batch_set_sweep(b, bs, bz);
     const int bchoices[4] = {1, 2, 4, 0};
-    for (int i = 0; i < 4 && rc == TMX_OK; i++) {
-        if (bchoices[i] >= b->bound_fit) continue;  // the same grid as 0
-        rc = tmx_batch_set_boundary(b, bchoices[i]);
-        if (rc) break;
-        double ms = 0;
-        trial(ms);
-        if (rc == TMX_OK && ms < best) {
-            best = ms;
-            bb = bchoices[i];
+    for (int after = 0; after < (b->K->serial ? 1 : 2) && rc == TMX_OK; after++)
+        for (int i = 0; i < 4 && rc == TMX_OK; i++) {
+            if (bchoices[i] >= b->bound_fit) continue;  // the same grid as 0
+            rc = tmx_batch_set_boundary(b, bchoices[i], after);
+            if (rc) break;
+            double ms = 0;
+            trial(ms);
+            if (rc == TMX_OK && ms < best) {
+                best = ms;
+                bb = bchoices[i];
+                ba = after;
+            }
         }
-    }
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
     if (rc) return rc;
-    rc = tmx_batch_set_boundary(b, bb);
+    rc = tmx_batch_set_boundary(b, bb, ba);
     if (rc) return rc;
     // the trials advanced the mixers: start every one of them again
     TMX_CK(cudaStreamSynchronize(b->stream));
