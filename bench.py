@@ -328,6 +328,24 @@ def profile_traffic(form: str = "fp64") -> dict | None:
 
 
 # ---------------------------------------------------------------------------
+def pattern_ceiling(precision: int, nodes: int, achieved: float, device: int) -> dict | None:
+    """The ceiling of the interior kernel's own access pattern
+    (tmx_pattern_ceiling: the same bytes per lattice update in the same
+    layout, no arithmetic) over the nodes of one launch, and the kernel's
+    achieved bandwidth as a fraction of it; None where it cannot run."""
+    import tmixer_b200 as T
+
+    try:
+        pc = T.pattern_ceiling(precision, max(int(nodes), 3 * 32768), reps=10, device=device)
+    except T.TmxError:
+        return None
+    return {"gbs": pc["gbs"], "frac": achieved / pc["gbs"], "blocks_per_sm": pc["blocks_per_sm"],
+            "nodes": pc["nodes"],
+            "what": "the interior kernel's loads and stores (19 direction planes read at the upstream nodes and "
+                    "written at the node, FP16 also the moment record) with no arithmetic: what DRAM gives "
+                    "this 38-stream pattern, beside the plain copy's peak"}
+
+
 def run_ours(args, dist: Dist) -> dict | None:
     import torch
 
@@ -392,6 +410,8 @@ def run_ours(args, dist: Dist) -> dict | None:
                 "algorithmic_bytes_per_launch": main["bulk_bytes"],
                 "boundary_kernels_ms": main["bnd_ms"], "bulk_kernel_ms": main["bulk_ms"],
                 "step_effective_gbs": main["step_gbs"]}
+    roofline["pattern_ceiling"] = pattern_ceiling(T.PRECISIONS[args.form], main["bulk_nodes"], main["achieved"],
+                                                  dist.local_rank)
     # --- the other forms, for comparison (same workload) --------------------
     forms = {}
     if not args.no_forms:
@@ -402,6 +422,8 @@ def run_ours(args, dist: Dist) -> dict | None:
                            "bulk_gbs": m["achieved"], "bulk_frac": m["achieved"] / peaks["hbm_gbs"],
                            "bytes_per_lup": FORM_BYTES[form],
                            "interior_kernel": "sweep4:%d" % FP16_SHAPE[1] if form == "fp16" else "flat"}
+            pc = pattern_ceiling(T.PRECISIONS[form], m["bulk_nodes"], m["achieved"], dist.local_rank)
+            forms[form]["bulk_pattern_frac"] = pc["frac"] if pc else None
 
     # --- e2e: the configured solve through the public API ---------------
     e2e_steps = args.e2e_steps
@@ -537,6 +559,8 @@ def run_batched(args, dist: Dist, fp64_mlups: float, peaks: dict) -> dict:
     # shape the z wall faces (one at each end of every interior column)
     swept = B_shape["kernel"] != "flat"
     upd = sum(interior_nodes(s) * (s.nz / (s.nz - 2) if swept else 1) for s in specs)
+    int_gbs = upd * FORM_BYTES["fp16"] / (t_int / kt * 1e-3) / 1e9
+    int_pc = pattern_ceiling(T.TMX_FP16, upd, int_gbs, dist.local_rank)
     mlups = nodes * args.batched_steps / (ms * 1e-3) / 1e6
     bpl = FORM_BYTES["fp16"]
     gbs = mlups * 1e6 * bpl / 1e9
@@ -549,7 +573,8 @@ def run_batched(args, dist: Dist, fp64_mlups: float, peaks: dict) -> dict:
                              "what": "the interior kernel alone (%d timed steps, boundary kernels before it), "
                                      "%d nodes per launch x %d B" % (kt, int(upd), bpl),
                              "ms": t_int / kt, "achieved": upd * bpl / (t_int / kt * 1e-3) / 1e9,
-                             "frac": upd * bpl / (t_int / kt * 1e-3) / 1e9 / peaks["hbm_gbs"]},
+                             "frac": upd * bpl / (t_int / kt * 1e-3) / 1e9 / peaks["hbm_gbs"],
+                             "pattern_ceiling": int_pc},
                          "boundary_kernels_ms": t_bnd / kt},
             "tuned": tuned, "launch_shape": B_shape,
             "nonfinite_outlet_im": int(sum(1 for r in im for v in r if v != v)),

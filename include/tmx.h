@@ -242,6 +242,20 @@ int tmx_step_timed(tmx_handle *h, int nsteps, double *ms_bulk, double *ms_bounda
  * (ms).  Benchmark support; no counterpart in the reference. */
 int tmx_time_steps(tmx_handle *h, int nsteps, double *ms);
 
+/* The memory-traffic ceiling of the interior kernels' access pattern on
+ * device `device`: kernels that move exactly the bytes of a lattice update of
+ * form `precision` (the 19 direction planes read at the upstream neighbours
+ * and written at the node: FP64 1216 B, FP32 608 B, FP16 304 B plus the
+ * 32-byte moment record read and written = 368 B), in the forms' layouts,
+ * with no arithmetic, over an x-fastest box of at least `nodes` nodes (at
+ * least 3 x 32768, at most 2^30), ping-ponging two buffers as the step does.
+ * Tries 1, 2, 4 and 8 blocks of 256 threads per SM, `reps` timed launches
+ * each after 3 untimed ones, and returns the best rate in *gbs (GB/s of
+ * those bytes) and its blocks per SM.  Allocates and frees its own buffers.
+ * Benchmark support (the denominator beside the plain copy bandwidth); no
+ * counterpart in the reference. */
+int tmx_pattern_ceiling(int precision, long long nodes, int reps, int device, double *gbs, int *blocks_per_sm);
+
 /* Launch shape of the interior (bulk) kernel; no counterpart in the
  * reference.  kind TMX_SHAPE_FLAT: one thread per node over the flat node
  * range (every form; zchunk ignored).  The sweep shapes (FP16 form only):

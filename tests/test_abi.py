@@ -78,3 +78,11 @@ def test_create_without_device_fails_cleanly():
     with pytest.raises(T.TmxError) as e:
         T.Solver(T.w_layout(4, 0.05, 0.56, 0.6, 1e-3, 1.0))
     assert e.value.code == -3
+
+
+@pytest.mark.parametrize("prec,nodes,reps", [(7, 1 << 20, 5), (0, 1000, 5), (2, 1 << 31, 5), (1, 1 << 20, 0)])
+def test_pattern_ceiling_rejects_bad_arguments(prec, nodes, reps):
+    """Argument checks come before any CUDA call, so they hold without a GPU."""
+    with pytest.raises(T.TmxError) as e:
+        T.pattern_ceiling(prec, nodes, reps)
+    assert e.value.code == -1

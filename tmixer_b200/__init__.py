@@ -126,6 +126,7 @@ def lib() -> ctypes.CDLL:
     L.tmx_counts.argtypes = [vp, P(ctypes.c_longlong)]
     L.tmx_set_shape.argtypes = [vp, ip, ip]
     L.tmx_time_steps.argtypes = [vp, ip, P(dp)]
+    L.tmx_pattern_ceiling.argtypes = [ip, ctypes.c_longlong, ip, ip, P(dp), P(ip)]
     L.tmx_destroy.argtypes = [vp]
     L.tmx_destroy.restype = None
     LL = ctypes.c_longlong
@@ -242,6 +243,16 @@ def reference_case() -> CaseSpec:
     _check(lib().tmx_case_reference(ctypes.byref(c)))
     return CaseSpec.from_c(c, steps=100001)
 
+
+def pattern_ceiling(precision: int, nodes: int, reps: int = 20, device: int = 0) -> dict:
+    """The memory-traffic ceiling of the interior kernels' access pattern for
+    one form (tmx_pattern_ceiling): GB/s of the form's bytes per lattice
+    update, moved in its layout with no arithmetic, over at least ``nodes``
+    nodes; the best of 1, 2, 4 and 8 blocks per SM."""
+    g, b = ctypes.c_double(), ctypes.c_int()
+    _check(lib().tmx_pattern_ceiling(int(precision), int(nodes), int(reps), int(device), ctypes.byref(g),
+                                     ctypes.byref(b)))
+    return dict(gbs=g.value, blocks_per_sm=b.value, nodes=int(nodes), reps=int(reps))
 
 def w_layout(W: int, u_max: float, tau_f: float, tau_c: float, k: float, rho: float = 1.0,
              steps: int = 0, precision: int = TMX_FP64) -> CaseSpec:

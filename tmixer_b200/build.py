@@ -21,7 +21,7 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC"]
 # per-source contraction: the FP64 kernels and the host code keep every
 # operation separately rounded; the reduced-precision kernels may fuse
 SOURCES = {"tmx_kernels.cu": ["--fmad=false"], "tmx_api.cu": ["--fmad=false"], "tmx_kernels_lp.cu": ["--fmad=true"],
-           "tmx_batch.cu": ["--fmad=false"]}
+           "tmx_batch.cu": ["--fmad=false"], "tmx_probe.cu": []}
 # host-only C++ sources of the library (no device code)
 CXX_SOURCES = {"tmx_serve.cpp": [], "tmx_writers.cpp": []}
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall"]
