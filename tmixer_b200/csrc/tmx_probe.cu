@@ -106,13 +106,20 @@ __global__ void __launch_bounds__(kThreads) k_pattern_f16(const uint2* __restric
     }
 }
 
-// device buffers of one probe, freed on every return path
+// device buffers, stream and events of one probe, released on every return
+// path
 struct Buffers {
     void* p[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaStream_t st = nullptr;
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
     ~Buffers()
     {
+        if (st) cudaStreamSynchronize(st);
         for (void* q : p)
             if (q) cudaFree(q);
+        if (t0) cudaEventDestroy(t0);
+        if (t1) cudaEventDestroy(t1);
+        if (st) cudaStreamDestroy(st);
     }
 };
 
@@ -143,6 +150,9 @@ extern "C" int tmx_pattern_ceiling(int precision, long long nodes, int reps, int
     int sms = 0;
     TMX_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
     Buffers buf;
+    TMX_CK(cudaStreamCreateWithFlags(&buf.st, cudaStreamNonBlocking));
+    TMX_CK(cudaEventCreate(&buf.t0));
+    TMX_CK(cudaEventCreate(&buf.t1));
     const int nbuf = precision == TMX_FP16 ? 4 : 2;
     for (int i = 0; i < nbuf; i++) {
         const long long sz = i < 2 ? pbytes : 32 * ps;
@@ -150,13 +160,10 @@ extern "C" int tmx_pattern_ceiling(int precision, long long nodes, int reps, int
             cudaGetLastError();
             return fail(TMX_E_NOMEM, "tmx_pattern_ceiling: no room for %lld bytes", sz);
         }
-        TMX_CK(cudaMemset(buf.p[i], 0, sz));
+        TMX_CK(cudaMemsetAsync(buf.p[i], 0, sz, buf.st));
     }
-    cudaStream_t st;
-    TMX_CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-    cudaEvent_t t0, t1;
-    TMX_CK(cudaEventCreate(&t0));
-    TMX_CK(cudaEventCreate(&t1));
+    cudaStream_t st = buf.st;
+    cudaEvent_t t0 = buf.t0, t1 = buf.t1;
     // ping-pong between the two buffers, as the interior kernels' A-B pairs
     auto launch = [&](int grid, int r) {
         void* a = buf.p[r & 1];
@@ -192,9 +199,6 @@ extern "C" int tmx_pattern_ceiling(int precision, long long nodes, int reps, int
             best_bps = bps;
         }
     }
-    cudaEventDestroy(t0);
-    cudaEventDestroy(t1);
-    cudaStreamDestroy(st);
     if (rc) return rc;
     *gbs = best;
     if (blocks_per_sm) *blocks_per_sm = best_bps;
