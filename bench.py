@@ -625,19 +625,48 @@ def run_served(args, dist: Dist, batched_mlups: float, shape: dict) -> dict:
                       % (len(reqs), list(SERVED_W), BATCH_SEED + 1, args.served_max_steps, budget / 1e9)}
 
 
+def reference_cpu_samples(params: dict, samples: int, warm: int, budget_s: float) -> dict:
+    """The reference arm's timing: ``warm`` untimed and then ``samples``
+    timed samples of the reference's own OpenMP build on all of this host's
+    cores, one sample being m consecutive steps of the solve, m sized so that
+    the whole run fits ``budget_s`` (one process: steps 1 .. warm*m untimed,
+    the next samples*m timed)."""
+    from oracle import build_ref, oracle as O
+
+    binary = build_ref.binary_path("bench_w%d" % WORKLOAD["W"], params)
+    cores = os.cpu_count() or 1
+    if not os.path.exists(binary):
+        if os.path.exists(build_ref.REF_SRC):
+            binary = build_ref.build("bench_w%d" % WORKLOAD["W"], params)
+        else:
+            return {"error": "reference binary for this workload not built"}
+    _, _, t2 = O.run_ref(binary, 3, threads=cores, warmup=1)  # probe: 2 timed steps
+    per = max(t2 / 2.0, 1e-4)
+    m = int(max(1, min(REF_SAMPLE_STEPS, budget_s / ((samples + warm) * per))))
+    _, _, secs = O.run_ref(binary, (warm + samples) * m, threads=cores, warmup=warm * m)
+    value = case_nodes(params) * samples * m / secs / 1e6
+    return {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "seconds": secs,
+            "steps_per_sample": m,
+            "sample": "%d timed samples of %d steps each (steps %d..%d of the solve, after %d untimed samples) of "
+                      "the same W=%d mixer, reference OpenMP build (g++ -O2 -fopenmp), OMP_NUM_THREADS=%d: %.2f s"
+                      % (samples, m, warm * m + 1, (warm + samples) * m, warm, WORKLOAD["W"], cores, secs)}
+
+
 def run_reference(args, dist: Dist) -> dict | None:
     """The reference arm: the reference's own OpenMP build (oracle/_ref,
     compiled from its source) on this host's cores, for the same case and
-    config as our arm.  Nothing here loads the CUDA library: the case
+    config as our arm; each of its --warmup and --steps steps is a sample of
+    m reference steps.  Nothing here loads the CUDA library: the case
     constants come from w_layout_params."""
     if dist.rank != 0:
         return None
     params = workload_params()
-    r = reference_cpu_run(params, budget_s=args.ref_budget)
+    r = reference_cpu_samples(params, args.steps, args.warmup, budget_s=args.ref_budget)
     if "error" in r:
         return {"impl": "reference", "unavailable": r["error"]}
     return {"impl": "reference", "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": dist.world,
-            "steps": r["steps"], "warmup": 1, "ms_per_step": r["seconds"] / r["steps"] * 1e3,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["seconds"] / args.steps * 1e3,
+            "steps_per_sample": r["steps_per_sample"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "form": "the reference's OpenMP CPU build (FP64)", "config": config_dict(params, dist.world),
             "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": "reference",
