@@ -468,7 +468,10 @@ def run_ours(args, dist: Dist) -> dict | None:
                    "hbm_frac_step": nodes_ref * FORM_BYTES["fp64"] / (ms_ref / n_ref * 1e-3) / 1e9 / peaks["hbm_gbs"]}
 
     batched = served = None
-    if not args.no_batched:
+    # the batched and served forms are one-GPU configurations (minutes of
+    # work): measured at N=1 only, so that a scaling run holds its GPUs for
+    # the replicas' timed steps and not for N copies of the served loop
+    if not args.no_batched and dist.world == 1:
         fp64 = forms.get("fp64", {}).get("mlups") or (value if args.form == "fp64" else None)
         batched = run_batched(args, dist, fp64, peaks)
         if not args.no_served:
