@@ -104,3 +104,39 @@ def test_reference_arm_does_not_load_the_library():
     # the same config dict as our arm's (which builds it from the same params)
     assert r["config"] == json.loads(json.dumps(bench.config_dict(bench.workload_params(), 1)))
     assert r["config"]["fluid_nodes"] == 524288
+
+
+def test_reference_arm_line():
+    """`bench.py --impl reference` end to end on the CPU with a small budget:
+    one JSON line with the driver's steps and warmup, our arm's config,
+    metric and unit, an e2e object without copies, and no module or library
+    of the package loaded in its process."""
+    import json
+    import subprocess
+    import sys
+
+    from oracle import build_ref
+
+    binary = build_ref.binary_path("bench_w%d" % bench.WORKLOAD["W"], bench.workload_params())
+    if not os.path.exists(binary) and not os.path.exists(build_ref.REF_SRC):
+        pytest.skip("reference binary not built and reference source absent")
+    root = os.path.dirname(os.path.abspath(bench.__file__))
+    code = ("import sys, json, io, contextlib, bench\n"
+            "buf = io.StringIO()\n"
+            "with contextlib.redirect_stdout(buf):\n"
+            "    rc = bench.main(['--impl', 'reference', '--steps', '1', '--warmup', '3', '--ref-budget', '1'])\n"
+            "maps = open('/proc/self/maps').read()\n"
+            "print(json.dumps({'rc': rc, 'line': buf.getvalue().strip().splitlines()[-1],"
+            " 'mods': [m for m in sys.modules if m.startswith('tmixer_b200')], 'libtmx': 'libtmx' in maps}))\n")
+    out = subprocess.run([sys.executable, "-c", code], cwd=root, capture_output=True, text=True, check=True,
+                         timeout=600)
+    r = json.loads(out.stdout.strip().splitlines()[-1])
+    assert r["rc"] == 0 and r["mods"] == [] and r["libtmx"] is False
+    line = json.loads(r["line"])
+    assert line["impl"] == "reference" and "unavailable" not in line
+    assert (line["steps"], line["warmup"]) == (1, 3)
+    assert line["metric"] == bench.METRIC and line["unit"] == bench.UNIT and line["higher_is_better"] is True
+    assert line["config"] == json.loads(json.dumps(bench.config_dict(bench.workload_params(), 1)))
+    assert line["value"] > 0 and line["e2e"]["value"] == line["value"]
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
+    assert line["cpu_baseline"]["kind"] == "reference" and line["steps_per_sample"] >= 1
