@@ -262,7 +262,9 @@ int tmx_pattern_ceiling(int precision, long long nodes, int reps, int device, do
  * blocks of 32 x TY threads own tiles of as many nodes of one box and walk
  * them through zchunk planes (zchunk >= 1), the writers' moment records
  * staged in shared memory: TMX_SHAPE_SWEEP8 (TY 8), TMX_SHAPE_SWEEP4 (TY 4).
- * Every shape gives the same results bit for bit.  Default: TMX_SHAPE_FLAT. */
+ * Every shape gives the same results bit for bit.  Default: TMX_SHAPE_SWEEP4
+ * with zchunk 8 for the FP16 form (set by tmx_create), TMX_SHAPE_FLAT for the
+ * others. */
 #define TMX_SHAPE_FLAT 0
 #define TMX_SHAPE_SWEEP8 1
 #define TMX_SHAPE_SWEEP4 2

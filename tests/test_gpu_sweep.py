@@ -21,7 +21,8 @@ def _case(name):
 
 def _state(spec, shape, zchunk, steps):
     with T.Solver(spec) as s:
-        s.set_shape(shape, zchunk)
+        if shape is not None:  # None: the handle's default shape
+            s.set_shape(shape, zchunk)
         s.init()
         s.step(steps)
         fields = [s.field(b, f) for b in (0, 1) for f in T.FIELDS]
@@ -50,7 +51,8 @@ def test_sweep_equals_flat(gpu, name):
     spec = _spec(name)
     steps = 25
     want = _state(spec, T.SHAPE_FLAT, 8, steps)
-    for shape, zchunk in ((T.SHAPE_SWEEP8, 8), (T.SHAPE_SWEEP4, 3), (T.SHAPE_SWEEP8, 1), (T.SHAPE_SWEEP4, 1000)):
+    for shape, zchunk in ((None, 0), (T.SHAPE_SWEEP8, 8), (T.SHAPE_SWEEP4, 3), (T.SHAPE_SWEEP8, 1),
+                          (T.SHAPE_SWEEP4, 1000)):
         got = _state(spec, shape, zchunk, steps)
         assert _same(got, want), (name, shape, zchunk)
 

@@ -405,7 +405,8 @@ class Solver:
     def set_shape(self, kind: int, zchunk: int = 8) -> "Solver":
         """Launch shape of the interior kernel (tmx_set_shape): SHAPE_FLAT, or
         for the FP16 form a sweep shape (SHAPE_SWEEP8, SHAPE_SWEEP4) with zchunk
-        planes per tile.  Every shape gives the same bits."""
+        planes per tile.  Every shape gives the same bits.  Default: SHAPE_SWEEP4
+        with 8 planes for the FP16 form, SHAPE_FLAT for the others."""
         _check(lib().tmx_set_shape(self._h, int(kind), int(zchunk)))
         return self
 

